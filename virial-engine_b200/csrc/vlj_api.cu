@@ -1,0 +1,672 @@
+// C ABI of the single-box simulation (include/virial_lj.h): the B200 stand-in
+// for virial_particles::lennard_jones::LennardJones
+// (crates/virial-particles/src/lennard_jones.rs:334-1375).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "virial_lj.h"
+#include "vlj_common.h"
+#include "vlj_internal.cuh"
+#include "vlj_sim.h"
+
+using namespace vlj;
+
+namespace vlj {
+
+// lennard_jones.rs:435-440
+double scale_for(double magnitude) {
+    if (magnitude <= 0.0 || !std::isfinite(magnitude)) return 1.0;
+    return std::pow(2.0, std::floor(20.0 - std::log2(magnitude)));
+}
+
+vlj_status check_settings(const vlj_settings* st) {
+    if (!st) return fail(VLJ_INVALID_ARG, "settings is null");
+    for (int k = 0; k < 3; k++)
+        if (!(st->box_size[k] > 0.0) || !std::isfinite(st->box_size[k]))
+            return fail(VLJ_INVALID_ARG, "box side %d is not a positive finite number", k);
+    if (!(st->cutoff > 0.0) || !std::isfinite(st->cutoff))
+        return fail(VLJ_INVALID_ARG, "cutoff must be positive");
+    if (!(st->skin >= 0.0) || !std::isfinite(st->skin))
+        return fail(VLJ_INVALID_ARG, "skin must be non-negative");
+    if (!(st->dt > 0.0) || !std::isfinite(st->dt)) return fail(VLJ_INVALID_ARG, "dt must be positive");
+    const vlj_thermostat& t = st->thermostat;
+    switch (t.kind) {
+        case VLJ_THERMOSTAT_NONE: break;
+        case VLJ_THERMOSTAT_LANGEVIN:
+            if (!(t.temperature >= 0.0) || !(t.friction >= 0.0) || !std::isfinite(t.temperature) ||
+                !std::isfinite(t.friction))
+                return fail(VLJ_INVALID_ARG, "Langevin needs temperature >= 0 and friction >= 0");
+            break;
+        case VLJ_THERMOSTAT_NOSE_HOOVER:
+            if (!(t.temperature > 0.0) || !(t.period > 0.0))
+                return fail(VLJ_INVALID_ARG, "Nose-Hoover needs temperature > 0 and period > 0");
+            break;
+        default: return fail(VLJ_INVALID_ARG, "unknown thermostat kind %d", (int)t.kind);
+    }
+    return VLJ_OK;
+}
+
+// What LennardJones::new derives from the settings (lennard_jones.rs:450-560).
+// min_cells is 3 for the reference's 27-cell search.
+vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3], double cutoff,
+                    double skin, double dt, bool shifted_force, const vlj_thermostat& t,
+                    uint32_t profile_bins, Box& b) {
+    std::memset(&b, 0, sizeof b);
+    const double list_radius = cutoff + skin;
+    uint32_t cells[3];
+    for (int k = 0; k < 3; k++) {
+        b.box_f[k] = (float)box_size[k];
+        b.box[k] = (double)b.box_f[k];
+        double c = std::floor(b.box[k] / list_radius);
+        cells[k] = c < 0.0 ? 0u : (c > 4.0e9 ? 4000000000u : (uint32_t)c);
+    }
+    if (cells[0] < 3 || cells[1] < 3 || cells[2] < 3)
+        return fail(VLJ_BOX_TOO_SMALL,
+                    "the box must be at least three (cutoff + skin) wide on every axis");
+    while ((uint64_t)cells[0] * cells[1] * cells[2] > (1u << 20)) {
+        int longest = 0;
+        for (int k = 1; k < 3; k++)
+            if (cells[k] >= cells[longest]) longest = k;
+        cells[longest] -= 1;
+    }
+    for (int k = 0; k < 3; k++) {
+        b.cells[k] = cells[k];
+        b.cell_size_f[k] = (float)(b.box[k] / (double)cells[k]);
+        b.enc[k] = 4294967296.0 / b.box[k];
+        b.dec[k] = (float)(b.box[k] / 4294967296.0);
+    }
+    b.total_cells = cells[0] * cells[1] * cells[2];
+    const double volume = b.box[0] * b.box[1] * b.box[2];
+    const double density = (double)count / volume;
+    const double expected =
+        4.0 / 3.0 * 3.141592653589793 * (list_radius * list_radius * list_radius) * density;
+    b.capacity = (uint32_t)std::ceil(2.0 * expected + 32.0);
+    b.n = (uint32_t)count;
+
+    double kinetic = 0.0, speed = 0.0;
+    for (size_t i = 0; i < count; i++) {
+        double v2 = 0.0;
+        for (int k = 0; k < 3; k++) v2 += p[i].vel[k] * p[i].vel[k];
+        kinetic += 0.5 * v2;
+        speed += std::sqrt(v2);
+    }
+    double thermal = 0.0;
+    if (t.kind != VLJ_THERMOSTAT_NONE) thermal = 1.5 * t.temperature * (double)count;
+    double m = std::max(std::max(kinetic, thermal), (double)count);
+    b.energy_scale = (float)scale_for(m);
+    b.momentum_scale = (float)scale_for(std::max(speed, (double)count));
+
+    const double rc2 = cutoff * cutoff;
+    const double inv6 = 1.0 / (rc2 * rc2 * rc2);
+    b.shift = (float)(4.0 * (inv6 * inv6 - inv6));
+    b.force_shift = shifted_force ? (float)(24.0 * (2.0 * inv6 * inv6 - inv6) / cutoff) : 0.0f;
+    b.rc = (float)std::sqrt((double)(float)rc2);
+    b.rc2 = (float)rc2;
+    b.list_r2 = (float)(list_radius * list_radius);
+    b.half_skin2 = (float)(0.25 * skin * skin);
+    b.dt = dt;
+    b.half_dt = 0.5 * dt;
+    b.c1 = 1.0;
+    b.c2 = 0.0;
+    b.thermostat = t.kind;
+    if (t.kind == VLJ_THERMOSTAT_LANGEVIN) {
+        b.c1 = std::exp(-t.friction * dt);
+        b.c2 = std::sqrt((1.0 - b.c1 * b.c1) * t.temperature);
+        b.seed = t.seed;
+    }
+    b.near_count = 4;
+    b.drawn = VLJ_DRAWN_NEIGHBOURS;
+    b.reorder_every = 4;
+    b.profile_bins = profile_bins;
+    b.bin_width = (float)(b.box[2] / (double)std::max(profile_bins, 1u));
+    return VLJ_OK;
+}
+
+}  // namespace vlj
+
+#define CUDA_TRY(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(VLJ_CUDA_ERROR, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                        __FILE__, __LINE__);                                                \
+    } while (0)
+
+#define TRY(expr)                          \
+    do {                                   \
+        vlj_status s_ = (expr);            \
+        if (s_ != VLJ_OK) return s_;       \
+    } while (0)
+
+namespace {
+
+template <class T>
+vlj_status dalloc(vlj_sim* s, T** p, size_t count) {
+    void* q = nullptr;
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    CUDA_TRY(cudaMalloc(&q, bytes));
+    s->allocations.push_back(q);
+    CUDA_TRY(cudaMemset(q, 0, bytes));
+    *p = static_cast<T*>(q);
+    return VLJ_OK;
+}
+
+double rem_euclid(double x, double side) {
+    double r = std::fmod(x, side);
+    return r < 0.0 ? r + side : r;
+}
+
+// Positions (wrapped into the box) and velocities as structure-of-arrays
+// uploads; ids are the input order.
+vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
+    const size_t seg = s->arena.seg;
+    std::vector<double> x(3 * seg, 0.0), v(3 * seg, 0.0);
+    std::vector<uint32_t> id(seg, 0u);
+    for (size_t i = 0; i < count; i++) {
+        for (int k = 0; k < 3; k++) {
+            if (!std::isfinite(p[i].pos[k]) || !std::isfinite(p[i].vel[k]))
+                return fail(VLJ_INVALID_ARG, "particle %zu has a non-finite coordinate", i);
+            x[k * seg + i] = rem_euclid(p[i].pos[k], s->box.box[k]);
+            v[k * seg + i] = p[i].vel[k];
+        }
+        id[i] = (uint32_t)i;
+    }
+    CUDA_TRY(cudaMemcpyAsync(s->arena.x, x.data(), sizeof(double) * 3 * seg,
+                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.v, v.data(), sizeof(double) * 3 * seg,
+                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.id, id.data(), sizeof(uint32_t) * seg,
+                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
+vlj_status lists_now(vlj_sim* s) {
+    CUDA_TRY(launch_decide(s->arena, s->stream, 0));
+    CUDA_TRY(launch_rebuild(s->arena, s->stream));
+    return VLJ_OK;
+}
+
+// Fresh state from `p`: forced rebuild, then the first forces turn the given
+// velocities into ones half a kick behind (lennard_jones.rs:1080-1089).
+vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
+    TRY(upload_particles(s, p, count));
+    uint32_t one = 1u;
+    CUDA_TRY(cudaMemcpyAsync(&s->arena.ctrl[0].forced, &one, sizeof one, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(launch_decide(s->arena, s->stream, 0));
+    CUDA_TRY(launch_encode(s->arena, s->stream));
+    CUDA_TRY(launch_rebuild(s->arena, s->stream));
+    CUDA_TRY(launch_prime(s->arena, s->shifted_force, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
+vlj_status push_box(vlj_sim* s) {
+    CUDA_TRY(cudaMemcpyAsync(const_cast<Box*>(s->arena.boxes), &s->box, sizeof(Box),
+                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
+vlj_measurement decode(const vlj_sim* s, const Readback& r, uint64_t step) {
+    vlj_measurement m;
+    std::memset(&m, 0, sizeof m);
+    auto value = [](long long raw) { return (double)raw / 4294967296.0; };
+    const double es = (double)s->box.energy_scale, ms = (double)s->box.momentum_scale;
+    m.step = step;
+    m.time = (double)step * s->settings.dt;
+    m.kinetic = value(r.slots[0]) / es;
+    m.potential = value(r.slots[1]) / es;
+    m.virial = value(r.slots[2]) / es;
+    for (int k = 0; k < 3; k++) m.momentum[k] = value(r.slots[3 + k]) / ms;
+    m.count = s->n;
+    m.volume = s->box.box[0] * s->box.box[1] * s->box.box[2];
+    m.list_rebuilds = r.ctrl.rebuilds;
+    m.list_overflow = r.ctrl.overflow;
+    m.condensed = (uint32_t)std::llround(value(r.slots[6]));
+    m.thermostat_energy = 0.0;
+    return m;
+}
+
+vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
+    CUDA_TRY(cudaMemsetAsync(s->arena.accum, 0, sizeof(unsigned long long) * kSlots, s->stream));
+    TRY(lists_now(s));
+    CUDA_TRY(launch_measure(s->arena, s->shifted_force, canonical, s->stream));
+    if (slot >= 0) {
+        Readback* r = &s->ring[slot];
+        CUDA_TRY(cudaMemcpyAsync(r->slots, s->arena.accum, sizeof(r->slots), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        CUDA_TRY(cudaMemcpyAsync(&r->ctrl, s->arena.ctrl, sizeof(Control), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        CUDA_TRY(cudaEventRecord(s->ring_event[slot], s->stream));
+        s->ring_busy[slot] = true;
+        s->ring_step[slot] = s->steps;
+    }
+    return VLJ_OK;
+}
+
+}  // namespace
+
+vlj_sim::~vlj_sim() {
+    if (step_graph_exec) cudaGraphExecDestroy(step_graph_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    for (int k = 0; k < kRing; k++)
+        if (ring_event[k]) cudaEventDestroy(ring_event[k]);
+    if (ring) cudaFreeHost(ring);
+    for (void* p : allocations) cudaFree(p);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+vlj_status vlj_device_count(int* count) {
+    if (!count) return fail(VLJ_INVALID_ARG, "count is null");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return VLJ_OK;
+}
+
+vlj_status vlj_create(const vlj_particle* particles, size_t count, const vlj_settings* settings,
+                      void* stream, vlj_sim** out) {
+    clear_error();
+    if (!out) return fail(VLJ_INVALID_ARG, "out is null");
+    *out = nullptr;
+    if (!particles || count == 0) return fail(VLJ_INVALID_ARG, "no particles");
+    if (count >= (1ull << 31)) return fail(VLJ_INVALID_ARG, "at most 2^31 - 1 particles");
+    TRY(check_settings(settings));
+    int devices = 0;
+    vlj_device_count(&devices);
+    if (devices == 0) return fail(VLJ_NO_DEVICE, "no CUDA device is visible");
+    if (settings->thermostat.kind == VLJ_THERMOSTAT_NOSE_HOOVER)
+        return fail(VLJ_NOT_ENABLED, "the Nose-Hoover thermostat is not available in this build");
+
+    vlj_sim* s = new vlj_sim();
+    s->settings = *settings;
+    s->n = (uint32_t)count;
+    s->shifted_force = settings->shifted_force != 0;
+    vlj_status st = make_box(particles, count, settings->box_size, settings->cutoff,
+                             settings->skin, settings->dt, s->shifted_force, settings->thermostat,
+                             settings->profile_bins, s->box);
+    if (st != VLJ_OK) {
+        delete s;
+        return st;
+    }
+    st = sim_allocate(s, stream);
+    if (st == VLJ_OK) st = restart(s, particles, count);
+    if (st != VLJ_OK) {
+        delete s;
+        return st;
+    }
+    *out = s;
+    return VLJ_OK;
+}
+
+vlj_status vlj_destroy(vlj_sim* sim) {
+    if (!sim) return VLJ_OK;
+    if (sim->stream) cudaStreamSynchronize(sim->stream);
+    delete sim;
+    return VLJ_OK;
+}
+
+vlj_status vlj_step(vlj_sim* s, uint32_t steps) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    TRY(sim_enqueue_steps(s, steps));
+    s->steps += steps;
+    return VLJ_OK;
+}
+
+vlj_status vlj_run(vlj_sim* s, uint64_t steps) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    while (steps > 0) {
+        uint32_t batch = (uint32_t)std::min<uint64_t>(steps, 200);
+        TRY(vlj_step(s, batch));
+        steps -= batch;
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
+vlj_status vlj_measure(vlj_sim* s, int* accepted) {
+    if (!s || !accepted) return fail(VLJ_INVALID_ARG, "null argument");
+    *accepted = 0;
+    int slot = -1;
+    for (int k = 0; k < kRing; k++)
+        if (!s->ring_busy[k]) {
+            slot = k;
+            break;
+        }
+    if (slot < 0) return VLJ_OK;
+    TRY(enqueue_measure(s, false, slot));
+    *accepted = 1;
+    return VLJ_OK;
+}
+
+vlj_status vlj_poll(vlj_sim* s, vlj_measurement* out, size_t capacity, size_t* written) {
+    if (!s || !written) return fail(VLJ_INVALID_ARG, "null argument");
+    *written = 0;
+    std::vector<std::pair<uint64_t, int>> ready;
+    for (int k = 0; k < kRing; k++) {
+        if (!s->ring_busy[k]) continue;
+        cudaError_t e = cudaEventQuery(s->ring_event[k]);
+        if (e == cudaSuccess)
+            ready.push_back({s->ring_step[k], k});
+        else if (e != cudaErrorNotReady)
+            return fail(VLJ_CUDA_ERROR, "measurement read-back: %s", cudaGetErrorString(e));
+    }
+    std::sort(ready.begin(), ready.end());
+    size_t n = 0;
+    for (auto& r : ready) {
+        if (n >= capacity || !out) break;
+        out[n++] = decode(s, s->ring[r.second], r.first);
+        s->ring_busy[r.second] = false;
+    }
+    *written = n;
+    return VLJ_OK;
+}
+
+vlj_status vlj_measure_now(vlj_sim* s, vlj_measurement* out) {
+    if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
+    int accepted = 0;
+    TRY(vlj_measure(s, &accepted));
+    if (!accepted) return fail(VLJ_BUSY, "a measurement is already in flight");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    vlj_measurement buf[kRing];
+    size_t n = 0;
+    TRY(vlj_poll(s, buf, kRing, &n));
+    if (n == 0) return fail(VLJ_CUDA_ERROR, "the measurement did not finish");
+    *out = buf[n - 1];
+    return VLJ_OK;
+}
+
+vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
+    if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
+    TRY(enqueue_measure(s, true, -1));
+    const size_t seg = s->arena.seg;
+    std::vector<double> x(3 * seg), v(3 * seg);
+    std::vector<uint32_t> id(seg);
+    CUDA_TRY(cudaMemcpyAsync(x.data(), s->arena.x, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(v.data(), s->arena.vcanon, sizeof(double) * 3 * seg,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(id.data(), s->arena.id, sizeof(uint32_t) * seg,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t slot = 0; slot < s->n; slot++) {
+        uint32_t i = id[slot];
+        if (i >= s->n) return fail(VLJ_CUDA_ERROR, "corrupt particle id %u in slot %u", i, slot);
+        for (int k = 0; k < 3; k++) {
+            out[i].pos[k] = x[k * seg + slot];
+            out[i].vel[k] = v[k * seg + slot];
+        }
+    }
+    return VLJ_OK;
+}
+
+vlj_status vlj_write_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
+    if (!s || !p) return fail(VLJ_INVALID_ARG, "null argument");
+    if (count != s->n) return fail(VLJ_INVALID_ARG, "expected %u particles, got %zu", s->n, count);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return restart(s, p, count);
+}
+
+vlj_status vlj_count(const vlj_sim* s, uint32_t* count) {
+    if (!s || !count) return fail(VLJ_INVALID_ARG, "null argument");
+    *count = s->n;
+    return VLJ_OK;
+}
+
+vlj_status vlj_box_size(const vlj_sim* s, double out[3]) {
+    if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
+    for (int k = 0; k < 3; k++) out[k] = s->box.box[k];
+    return VLJ_OK;
+}
+
+vlj_status vlj_volume(const vlj_sim* s, double* volume) {
+    if (!s || !volume) return fail(VLJ_INVALID_ARG, "null argument");
+    *volume = s->box.box[0] * s->box.box[1] * s->box.box[2];
+    return VLJ_OK;
+}
+
+vlj_status vlj_steps(const vlj_sim* s, uint64_t* steps) {
+    if (!s || !steps) return fail(VLJ_INVALID_ARG, "null argument");
+    *steps = s->steps;
+    return VLJ_OK;
+}
+
+vlj_status vlj_time(const vlj_sim* s, double* time) {
+    if (!s || !time) return fail(VLJ_INVALID_ARG, "null argument");
+    *time = (double)s->steps * s->settings.dt;
+    return VLJ_OK;
+}
+
+vlj_status vlj_target_temperature(const vlj_sim* s, int* has, double* temperature) {
+    if (!s || !has || !temperature) return fail(VLJ_INVALID_ARG, "null argument");
+    *has = s->settings.thermostat.kind != VLJ_THERMOSTAT_NONE;
+    *temperature = *has ? s->settings.thermostat.temperature : 0.0;
+    return VLJ_OK;
+}
+
+vlj_status vlj_positions(const vlj_sim* s, const double** xyz, size_t* stride) {
+    if (!s || !xyz || !stride) return fail(VLJ_INVALID_ARG, "null argument");
+    *xyz = s->arena.x;
+    *stride = s->arena.seg;
+    return VLJ_OK;
+}
+
+vlj_status vlj_velocities(const vlj_sim* s, const float** vel4) {
+    if (!s || !vel4) return fail(VLJ_INVALID_ARG, "null argument");
+    *vel4 = reinterpret_cast<const float*>(s->arena.vel4);
+    return VLJ_OK;
+}
+
+vlj_status vlj_set_drawn(vlj_sim* s, vlj_drawn drawn) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (drawn != VLJ_DRAWN_NEIGHBOURS && drawn != VLJ_DRAWN_TEMPERATURE)
+        return fail(VLJ_INVALID_ARG, "unknown drawn value %d", (int)drawn);
+    s->box.drawn = (uint32_t)drawn;
+    return push_box(s);
+}
+
+vlj_status vlj_set_condensed_neighbours(vlj_sim* s, uint32_t neighbours) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    s->box.near_count = neighbours;
+    return push_box(s);
+}
+
+// lennard_jones.rs:905-925
+vlj_status vlj_set_temperature(vlj_sim* s, double temperature) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (!(temperature >= 0.0) || !std::isfinite(temperature))
+        return fail(VLJ_INVALID_ARG, "temperature must be a non-negative number");
+    vlj_thermostat& t = s->settings.thermostat;
+    if (t.kind == VLJ_THERMOSTAT_NONE)
+        return fail(VLJ_NOT_ENABLED, "set_temperature needs a thermostat");
+    t.temperature = temperature;
+    if (t.kind == VLJ_THERMOSTAT_LANGEVIN) {
+        double c1 = std::exp(-t.friction * s->settings.dt);
+        s->box.c2 = std::sqrt((1.0 - c1 * c1) * temperature);
+    }
+    return push_box(s);
+}
+
+vlj_status vlj_set_heat_exchange(vlj_sim* s, const vlj_heat_exchange* exchange) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (s->settings.thermostat.kind != VLJ_THERMOSTAT_NONE)
+        return fail(VLJ_NOT_ENABLED, "heat exchange runs at constant energy, without a thermostat");
+    (void)exchange;
+    return fail(VLJ_NOT_ENABLED, "heat exchange is not available in this build");
+}
+
+vlj_status vlj_heat_flux(const vlj_sim* s, int* has, double* flux) {
+    if (!s || !has || !flux) return fail(VLJ_INVALID_ARG, "null argument");
+    *has = 0;
+    *flux = 0.0;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_grid_info(vlj_sim* s, vlj_grid_info* info) {
+    if (!s || !info) return fail(VLJ_INVALID_ARG, "null argument");
+    Control c;
+    CUDA_TRY(cudaMemcpyAsync(&c, s->arena.ctrl, sizeof c, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 3; k++) {
+        info->cells[k] = s->box.cells[k];
+        info->cell_size[k] = s->box.cell_size_f[k];
+    }
+    info->total_cells = s->box.total_cells;
+    info->capacity = s->box.capacity;
+    info->segment = s->arena.seg;
+    info->rebuilds = c.rebuilds;
+    info->reorder_every = s->box.reorder_every;
+    info->list_r2 = s->box.list_r2;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_read_grid(vlj_sim* s, uint32_t* sorted, uint32_t* cell_start,
+                               uint32_t* cell_of_slot, uint32_t* ids, uint32_t* list_count,
+                               uint32_t* list, double* pos, double* vel_stored) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    const size_t n = s->n, seg = s->arena.seg, cap = s->box.capacity;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    auto get = [&](void* dst, const void* src, size_t bytes) -> vlj_status {
+        if (!dst) return VLJ_OK;
+        CUDA_TRY(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return VLJ_OK;
+    };
+    TRY(get(sorted, s->arena.sorted, sizeof(uint32_t) * n));
+    TRY(get(cell_start, s->arena.cell_start, sizeof(uint32_t) * (s->box.total_cells + 1)));
+    TRY(get(cell_of_slot, s->arena.cell_of_slot, sizeof(uint32_t) * n));
+    TRY(get(ids, s->arena.id, sizeof(uint32_t) * n));
+    TRY(get(list_count, s->arena.list_count, sizeof(uint32_t) * n));
+    if (list) {
+        std::vector<uint32_t> t(seg * cap);
+        TRY(get(t.data(), s->arena.list, sizeof(uint32_t) * seg * cap));
+        for (size_t i = 0; i < n; i++)
+            for (size_t k = 0; k < cap; k++) list[i * cap + k] = t[k * seg + i];
+    }
+    if (pos || vel_stored) {
+        std::vector<double> x(3 * seg), v(3 * seg);
+        TRY(get(x.data(), s->arena.x, sizeof(double) * 3 * seg));
+        TRY(get(v.data(), s->arena.v, sizeof(double) * 3 * seg));
+        for (size_t i = 0; i < n; i++)
+            for (int k = 0; k < 3; k++) {
+                if (pos) pos[3 * i + k] = x[k * seg + i];
+                if (vel_stored) vel_stored[3 * i + k] = v[k * seg + i];
+            }
+    }
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_force_rebuild(vlj_sim* s) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    uint32_t one = 1u;
+    CUDA_TRY(cudaMemcpyAsync(&s->arena.ctrl[0].forced, &one, sizeof one, cudaMemcpyHostToDevice,
+                             s->stream));
+    TRY(lists_now(s));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_read_partials(vlj_sim* s, float* pe_half, float* w_half, int64_t* raw) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (pe_half)
+        CUDA_TRY(cudaMemcpy(pe_half, s->arena.pe_half, sizeof(float) * s->n, cudaMemcpyDeviceToHost));
+    if (w_half)
+        CUDA_TRY(cudaMemcpy(w_half, s->arena.w_half, sizeof(float) * s->n, cudaMemcpyDeviceToHost));
+    if (raw)
+        CUDA_TRY(cudaMemcpy(raw, s->arena.accum, sizeof(int64_t) * kSlots, cudaMemcpyDeviceToHost));
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_launches(uint64_t* n) {
+    if (!n) return fail(VLJ_INVALID_ARG, "null argument");
+    *n = launches();
+    return VLJ_OK;
+}
+
+}  // extern "C"
+
+// ---- allocation and step enqueue (shared with the graph path) ----
+namespace vlj {
+
+vlj_status sim_allocate(vlj_sim* s, void* stream) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    s->device = dev;
+    if (stream) {
+        s->stream = static_cast<cudaStream_t>(stream);
+        s->own_stream = false;
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    Arena& a = s->arena;
+    std::memset(&a, 0, sizeof a);
+    const uint32_t n = s->n;
+    const uint32_t seg = (n + 15u) / 16u * 16u;  // lennard_jones.rs:470
+    a.nboxes = 1;
+    a.nslots = n;
+    a.seg = seg;
+    a.ncells = s->box.total_cells;
+    s->box.first = 0;
+    s->box.cell_base = 0;
+    Box* d_box = nullptr;
+    TRY(dalloc(s, &d_box, 1));
+    a.boxes = d_box;
+    TRY(dalloc(s, &a.ctrl, 1));
+    TRY(dalloc(s, &a.glob, 1));
+    TRY(dalloc(s, &a.x, 3 * (size_t)seg));
+    TRY(dalloc(s, &a.v, 3 * (size_t)seg));
+    TRY(dalloc(s, &a.id, seg));
+    TRY(dalloc(s, &a.cache[0], seg));
+    TRY(dalloc(s, &a.cache[1], seg));
+    TRY(dalloc(s, &a.snap, seg));
+    TRY(dalloc(s, &a.ref, seg));
+    TRY(dalloc(s, &a.ref_lo, seg));
+    TRY(dalloc(s, &a.cell_of_slot, seg));
+    TRY(dalloc(s, &a.sorted, seg));
+    TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));
+    TRY(dalloc(s, &a.count, a.ncells));
+    TRY(dalloc(s, &a.list_count, seg));
+    TRY(dalloc(s, &a.list, (size_t)seg * s->box.capacity));
+    TRY(dalloc(s, &a.sx, 3 * (size_t)seg));
+    TRY(dalloc(s, &a.sv, 3 * (size_t)seg));
+    TRY(dalloc(s, &a.sid, seg));
+    TRY(dalloc(s, &a.scell, seg));
+    TRY(dalloc(s, &a.accum, kSlots));
+    TRY(dalloc(s, &a.pe_half, seg));
+    TRY(dalloc(s, &a.w_half, seg));
+    TRY(dalloc(s, &a.vel4, seg));
+    TRY(dalloc(s, &a.vcanon, 3 * (size_t)seg));
+    // the last cell of the box ends at the last slot
+    CUDA_TRY(cudaMemcpy(a.cell_start + a.ncells, &n, sizeof n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_box, &s->box, sizeof(Box), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMallocHost(&s->ring, sizeof(Readback) * kRing));
+    for (int k = 0; k < kRing; k++) {
+        CUDA_TRY(cudaEventCreateWithFlags(&s->ring_event[k], cudaEventDisableTiming));
+        s->ring_busy[k] = false;
+    }
+    return VLJ_OK;
+}
+
+vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
+    for (uint32_t k = 0; k < steps; k++) {
+        CUDA_TRY(launch_decide(s->arena, s->stream, 0));
+        CUDA_TRY(launch_rebuild(s->arena, s->stream));
+        CUDA_TRY(launch_step(s->arena, s->shifted_force, s->stream));
+    }
+    return VLJ_OK;
+}
+
+}  // namespace vlj

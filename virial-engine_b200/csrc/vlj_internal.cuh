@@ -1,0 +1,253 @@
+// Internal structures and device helpers of the B200 Lennard-Jones library.
+//
+// Layout in HBM (one "arena" holds one box, or many independent boxes for the
+// batched path, each box a contiguous run of slots and of cells):
+//   x, v      f64, structure of arrays: x[k * seg + slot], k = 0, 1, 2.
+//             v is stored half a kick behind (see the step kernel), so one
+//             force pass serves the closing half kick of a step and the
+//             opening half kick of the next.
+//   cache[2]  uint4 per slot: the position as 32-bit fractions of the box
+//             (X = round(x / L * 2^32) mod 2^32). Two copies: the step kernel
+//             reads one and writes the other; `phase` says which is current.
+//             Differences of these words wrap modulo 2^32, which is the
+//             minimum image for free, at 32-bit resolution on any box size.
+//   snap      uint4 per slot: the cache word at the last list build, for the
+//             skin / 2 displacement trigger.
+//   ref       float4 per slot, written at each rebuild: the reference's
+//             packed position (f32 hi in xyz, lo as three 9-bit fractions of
+//             the hi part's last bit in w) and ref_lo (the full f32 lo part).
+//             The list build uses exactly the reference's f32 predicate on
+//             these, so lists match it bit for bit.
+//   list      u32, transposed: entry k of slot i at list[k * seg + i];
+//             counts in list_count[i].
+//   cells     per cell: count (atomic cursor) and start. Boxes own contiguous
+//             runs of slots and cells, so one start array of ncells + 1 entries
+//             serves every box: box b's last cell ends where box b + 1 begins.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vlj {
+
+constexpr int kBlock = 256;
+constexpr int kSlots = 8;  // measurement accumulators per box
+// measurement slots: 0 kinetic, 1 potential, 2 virial, 3-5 momentum,
+// 6 condensed count, 7 unused (lennard_jones.wgsl:576-626)
+
+// Constants of one box. Read by every kernel from device memory, so a
+// setter changes them without re-capturing graphs.
+struct Box {
+    double box[3];       // sides, rounded to f32 (lennard_jones.rs:450)
+    double enc[3];       // 2^32 / side
+    double dt, half_dt;
+    double c1, c2;       // Langevin v <- c1 v + c2 xi (lennard_jones.rs:520-523)
+    float dec[3];        // side / 2^32, exact in f32
+    float box_f[3];
+    float cell_size_f[3];
+    float rc2, list_r2, half_skin2;
+    float shift, force_shift, rc;
+    float energy_scale, momentum_scale;
+    float bin_width;
+    uint32_t cells[3];
+    uint32_t total_cells;
+    uint32_t cell_base;  // first cell of this box
+    uint32_t first;      // first slot of this box
+    uint32_t n;
+    uint32_t capacity;   // list entries per particle
+    int32_t thermostat;  // 0 constant energy, 1 Langevin, 2 Nose-Hoover
+    uint32_t seed;
+    uint32_t near_count;
+    uint32_t drawn;
+    uint32_t reorder_every;
+    uint32_t profile_bins;
+    uint32_t pad[2];
+};
+
+// Mutable per-box words.
+struct Control {
+    uint32_t max_disp;   // f32 bits of the largest squared displacement
+    uint32_t rebuild;    // this step rebuilds
+    uint32_t reorder;    // this rebuild also moves particles into cell order
+    uint32_t rebuilds;   // rebuilds so far (lennard_jones.wgsl:299-305)
+    uint32_t overflow;   // largest neighbour count that did not fit
+    uint32_t built;      // 0 until the first build
+    uint32_t forced;     // rebuild at the next decision whatever moved
+    uint32_t pad;
+};
+
+// Words shared by every box of an arena.
+struct Global {
+    uint32_t phase;      // which cache copy holds the current positions
+    uint32_t pending;    // a step finished since the last decision
+    uint32_t any;        // some box rebuilds this step
+    uint32_t fault;      // first error a kernel recorded (0 none)
+    unsigned long long step;  // steps taken: the counter of the noise stream
+};
+
+// Every pointer a kernel needs; passed by value (it sits in the constant
+// bank), so captured graphs see fixed pointers and read the mutable state
+// through Control and Global.
+struct Arena {
+    const Box* boxes;
+    Control* ctrl;
+    Global* glob;
+    uint32_t nboxes;
+    uint32_t nslots;     // particles in all boxes
+    uint32_t seg;        // padded slot count (list row length)
+    uint32_t ncells;     // cells in all boxes
+    const uint32_t* box_of_slot;  // null for a single box
+    const uint32_t* box_of_cell;  // null for a single box
+    double* x;
+    double* v;
+    uint32_t* id;
+    uint4* cache[2];
+    uint4* snap;
+    float4* ref;
+    float4* ref_lo;
+    uint32_t* cell_of_slot;
+    uint32_t* sorted;
+    uint32_t* cell_start;  // ncells + 1
+    uint32_t* count;
+    uint32_t* list_count;
+    uint32_t* list;
+    // reorder scratch
+    double* sx;
+    double* sv;
+    uint32_t* sid;
+    uint32_t* scell;
+    // measurements
+    unsigned long long* accum;  // nboxes * kSlots
+    float* pe_half;
+    float* w_half;
+    float4* vel4;
+    double* vcanon;             // canonical velocities (3 * seg), on request
+    // profiles / heat current
+    unsigned long long* profile;  // bins * 8 + 3 per box
+    unsigned long long* series;   // 1 + 3 * capacity
+    uint32_t series_capacity;
+};
+
+// ---- fixed point: 32.32, round to nearest even ----
+// For f32 x with |x| < 2^31 this equals the reference's integer split
+// (fixed.wgsl:20-55): x * 2^32 is exact in f64 and the conversion rounds to
+// nearest even.
+__device__ __forceinline__ long long fixed_raw_f32(float x) {
+    return __double2ll_rn((double)x * 4294967296.0);
+}
+__device__ __forceinline__ long long fixed_raw_f64(double x) {
+    return __double2ll_rn(x * 4294967296.0);
+}
+
+// ---- position encoding ----
+__device__ __forceinline__ uint32_t encode(double x, double enc) {
+    return (uint32_t)(unsigned long long)__double2ll_rn(x * enc);
+}
+__device__ __forceinline__ float decode_diff(uint32_t a, uint32_t b, float dec) {
+    return (float)(int32_t)(a - b) * dec;
+}
+
+// ---- the reference's packed positions (lennard_jones.wgsl:128-152), IEEE
+// f32 operations exactly as written (no contraction) ----
+__device__ __forceinline__ float last_bit(float h) {
+    uint32_t e = (__float_as_uint(h) >> 23) & 0xffu;
+    e = e < 24u ? 24u : e;
+    return __uint_as_float((e - 23u) << 23);
+}
+
+__device__ __forceinline__ uint32_t pack_lo(float3 hi, float3 lo) {
+    uint32_t bits = 0x20000000u;
+    float h[3] = {hi.x, hi.y, hi.z};
+    float l[3] = {lo.x, lo.y, lo.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float t = __fdiv_rn(l[k], last_bit(h[k]));
+        t = fminf(fmaxf(t, -0.5f), 0.5f);
+        int32_t q = (int32_t)rintf(__fmul_rn(t, 510.0f));
+        bits |= (uint32_t)(q + 256) << (9u * (uint32_t)k);
+    }
+    return bits;
+}
+
+__device__ __forceinline__ float unpack_lo1(float h, uint32_t bits, int k) {
+    float q = (float)((int32_t)((bits >> (9u * (uint32_t)k)) & 511u) - 256);
+    return __fmul_rn(__fdiv_rn(q, 510.0f), last_bit(h));
+}
+
+// nearest image, lennard_jones.wgsl:199-202
+__device__ __forceinline__ float nearest_ref(float d, float side) {
+    return __fsub_rn(d, __fmul_rn(side, rintf(__fdiv_rn(d, side))));
+}
+
+// ---- Philox-4x32-10 (Salmon et al., SC'11), counter (id, step lo, step hi,
+// 0), key (seed, "LJV1") ----
+__device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, uint32_t seed) {
+    uint32_t c0 = id, c1 = (uint32_t)step, c2 = (uint32_t)(step >> 32), c3 = 0u;
+    uint32_t k0 = seed, k1 = 0x4C4A5631u;
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+// Three gaussians: uniforms in (0, 1] from 24 bits (as the reference's
+// uniform01, lennard_jones.wgsl:175-178), Box-Muller in f32.
+__device__ __forceinline__ float3 langevin_noise(uint32_t id, unsigned long long step,
+                                                 uint32_t seed) {
+    uint4 r = philox(id, step, seed);
+    float u0 = __fdiv_rn((float)(r.x >> 8) + 1.0f, 16777216.0f);
+    float u1 = __fdiv_rn((float)(r.y >> 8) + 1.0f, 16777216.0f);
+    float u2 = __fdiv_rn((float)(r.z >> 8) + 1.0f, 16777216.0f);
+    float u3 = __fdiv_rn((float)(r.w >> 8) + 1.0f, 16777216.0f);
+    float ra = sqrtf(-2.0f * logf(u0));
+    float aa = 6.283185307179586f * u1;
+    float rb = sqrtf(-2.0f * logf(u2));
+    float ab = 6.283185307179586f * u3;
+    return make_float3(ra * cosf(aa), ra * sinf(aa), rb * cosf(ab));
+}
+
+// r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545)
+template <bool SHIFTED_FORCE>
+__device__ __forceinline__ void lj_pair(float r2, const Box& b, float& rf, float& u) {
+    float inv2 = 1.0f / r2;
+    float s6 = inv2 * inv2 * inv2;
+    float s12 = s6 * s6;
+    rf = 24.0f * (2.0f * s12 - s6);
+    u = 4.0f * (s12 - s6) - b.shift;
+    if (SHIFTED_FORCE) {
+        float r = sqrtf(r2);
+        rf -= r * b.force_shift;
+        u += (r - b.rc) * b.force_shift;
+    }
+}
+
+template <bool SHIFTED_FORCE>
+__device__ __forceinline__ float lj_force_over_r2(float r2, const Box& b) {
+    float inv2 = 1.0f / r2;
+    float s6 = inv2 * inv2 * inv2;
+    float rf = 24.0f * s6 * (2.0f * s6 - 1.0f);
+    if (SHIFTED_FORCE) rf -= sqrtf(r2) * b.force_shift;
+    return rf * inv2;
+}
+
+// ---- launchers (vlj_kernels.cu); every kernel takes the Arena by value ----
+cudaError_t launch_encode(const Arena& a, cudaStream_t s);
+cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle);
+cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
+cudaError_t launch_prime(const Arena& a, bool shifted_force, cudaStream_t s);
+cudaError_t launch_step(const Arena& a, bool shifted_force, cudaStream_t s);
+cudaError_t launch_measure(const Arena& a, bool shifted_force, bool canonical, cudaStream_t s);
+cudaError_t launch_profile(const Arena& a, bool shifted_force, cudaStream_t s);
+cudaError_t launch_heat_current(const Arena& a, bool shifted_force, cudaStream_t s);
+unsigned long long launches();
+
+}  // namespace vlj

@@ -1,0 +1,646 @@
+// CUDA kernels of the Lennard-Jones step for sm_100a.
+//
+// One step is: decide (one block: flip the position copy, decide which boxes
+// rebuild) -> rebuild chain (bin, scan, scatter, per-cell sort with optional
+// reorder, copy back, pack, list build; every kernel returns at once unless
+// some box rebuilds, and inside a CUDA graph the chain sits under a
+// conditional node so it is not launched at all) -> the fused step kernel
+// (forces from the Verlet list, a full kick, the drift with Langevin friction
+// and noise, re-encoding, and the displacement trigger). Reference kernels
+// this follows are cited at each kernel.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launches() { return g_launches.load(); }
+
+static cudaError_t after_launch(unsigned n = 1) {
+    g_launches += n;
+    return cudaGetLastError();
+}
+
+static unsigned blocks_for(uint32_t n, int threads = kBlock) {
+    unsigned b = (n + threads - 1) / threads;
+    return b ? b : 1;
+}
+
+__device__ __forceinline__ uint32_t box_of_slot(const Arena& a, uint32_t slot) {
+    return a.box_of_slot ? a.box_of_slot[slot] : 0u;
+}
+
+__device__ __forceinline__ uint32_t box_of_cell(const Arena& a, uint32_t cell) {
+    return a.box_of_cell ? a.box_of_cell[cell] : 0u;
+}
+
+__device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
+    return a.ctrl[b].rebuild != 0u;
+}
+
+// Largest value over the block, one atomicMax per box present: all lanes of a
+// block normally belong to one box; blocks that straddle boxes fall back to
+// one atomic per lane.
+__device__ __forceinline__ void block_max_per_box(const Arena& a, bool valid, uint32_t b,
+                                                  float value) {
+    __shared__ uint32_t s_val[kBlock / 32];
+    __shared__ uint32_t s_box[kBlock / 32 + 1];
+    __shared__ int s_mixed;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t bits = valid ? __float_as_uint(value) : 0u;
+    uint32_t myb = valid ? b : 0xffffffffu;
+    if (threadIdx.x == 0) s_mixed = 0;
+    __syncthreads();
+    // box of the block's first valid lane
+    if (threadIdx.x == 0) s_box[kBlock / 32] = box_of_slot(a, blockIdx.x * blockDim.x);
+    __syncthreads();
+    uint32_t ref = s_box[kBlock / 32];
+    if (valid && myb != ref) s_mixed = 1;
+    __syncthreads();
+    if (s_mixed) {
+        if (valid) atomicMax(&a.ctrl[b].max_disp, bits);
+        return;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bits = max(bits, __shfl_xor_sync(0xffffffffu, bits, o));
+    if (lane == 0) s_val[warp] = bits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = max(m, s_val[w]);
+        atomicMax(&a.ctrl[ref].max_disp, m);
+    }
+}
+
+// Sum of kSlots 64-bit integers over the block into the box's accumulators;
+// same box-uniform shortcut as above.
+__device__ __forceinline__ void block_sum_slots(const Arena& a, bool valid, uint32_t b,
+                                                long long (&v)[kSlots]) {
+    __shared__ long long s_sum[kBlock / 32][kSlots];
+    __shared__ uint32_t s_ref;
+    __shared__ int s_mixed;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_mixed = 0;
+        s_ref = box_of_slot(a, blockIdx.x * blockDim.x);
+    }
+    __syncthreads();
+    if (valid && b != s_ref) s_mixed = 1;
+    __syncthreads();
+    if (s_mixed) {
+        if (valid)
+            for (int k = 0; k < kSlots; k++)
+                if (v[k]) atomicAdd(&a.accum[b * kSlots + k], (unsigned long long)v[k]);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kSlots; k++) {
+        long long x = valid ? v[k] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) s_sum[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kSlots) {
+        long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_sum[w][threadIdx.x];
+        if (t) atomicAdd(&a.accum[s_ref * kSlots + threadIdx.x], (unsigned long long)t);
+    }
+}
+
+// ---- encode positions into the current cache copy ----
+__global__ void encode_kernel(Arena a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[box_of_slot(a, i)];
+    uint4 w;
+    w.x = encode(a.x[i], bx.enc[0]);
+    w.y = encode(a.x[a.seg + i], bx.enc[1]);
+    w.z = encode(a.x[2 * a.seg + i], bx.enc[2]);
+    w.w = 0u;
+    a.cache[a.glob->phase][i] = w;
+}
+
+// ---- decide (lennard_jones.wgsl:281-307) ----
+// One block. Finishes the previous step's bookkeeping (flip the position
+// copy, advance the step counter), then per box: rebuild when something moved
+// more than skin / 2 since the last build, or never built; reorder on every
+// reorder_every-th rebuild (counted before the increment, as the reference).
+template <bool SET_CONDITION>
+__global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
+    __shared__ int s_any;
+    Global* g = a.glob;
+    if (threadIdx.x == 0) {
+        s_any = 0;
+        if (g->pending) {
+            g->phase ^= 1u;
+            g->step += 1ull;
+            g->pending = 0u;
+        }
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < a.nboxes; b += blockDim.x) {
+        Control& c = a.ctrl[b];
+        const Box& bx = a.boxes[b];
+        float moved = __uint_as_float(c.max_disp);
+        c.max_disp = 0u;
+        bool rebuild = moved > bx.half_skin2 || c.built == 0u || c.forced != 0u;
+        c.forced = 0u;
+        c.rebuild = rebuild ? 1u : 0u;
+        if (rebuild) {
+            c.reorder = (c.rebuilds % bx.reorder_every == 0u) ? 1u : 0u;
+            c.rebuilds += 1u;
+            c.built = 1u;
+            s_any = 1;
+        } else {
+            c.reorder = 0u;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g->any = (uint32_t)s_any;
+        if (SET_CONDITION) cudaGraphSetConditional(handle, (unsigned)s_any);
+    }
+}
+
+// ---- bin (grid.wgsl:11-38): cell of each slot from its f32 position ----
+__global__ void bin_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    uint32_t b = box_of_slot(a, i);
+    if (!rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    int32_t c[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float hi = (float)a.x[k * a.seg + i];
+        int32_t v = (int32_t)floorf(__fdiv_rn(hi, bx.cell_size_f[k]));
+        int32_t m = (int32_t)bx.cells[k] - 1;
+        c[k] = v < 0 ? 0 : (v > m ? m : v);
+    }
+    uint32_t cell =
+        bx.cell_base + ((uint32_t)c[2] * bx.cells[1] + (uint32_t)c[1]) * bx.cells[0] + (uint32_t)c[0];
+    a.cell_of_slot[i] = cell;
+    atomicAdd(&a.count[cell], 1u);
+}
+
+// ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
+// the counts offset by the box's first slot; counts become zeroed cursors.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t b = blockIdx.x;
+    if (b >= a.nboxes || !rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    __shared__ uint32_t s_carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_carry = bx.first;
+    __syncthreads();
+    const uint32_t total = bx.total_cells, base = bx.cell_base;
+    for (uint32_t tile = 0; tile < total; tile += kScanThreads * kScanPer) {
+        uint32_t v[kScanPer];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) {
+            uint32_t c = tile + threadIdx.x * kScanPer + q;
+            v[q] = c < total ? a.count[base + c] : 0u;
+            sum += v[q];
+        }
+        // inclusive scan of the per-thread sums
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += t;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        uint32_t before = s_carry + (warp ? s_warp[warp - 1] : 0u) + incl - sum;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) {
+            uint32_t c = tile + threadIdx.x * kScanPer + q;
+            if (c < total) {
+                a.cell_start[base + c] = before;
+                a.count[base + c] = 0u;
+            }
+            before += v[q];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += s_warp[kScanThreads / 32 - 1];
+        __syncthreads();
+    }
+}
+
+// ---- scatter (grid.wgsl:119-127): slot into its cell's next free place ----
+__global__ void scatter_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    if (!rebuilding(a, box_of_slot(a, i))) return;
+    uint32_t c = a.cell_of_slot[i];
+    a.sorted[a.cell_start[c] + atomicAdd(&a.count[c], 1u)] = i;
+}
+
+// ---- per-cell order (grid.wgsl:129-148) ----
+// One warp per cell: each slot's rank is the number of smaller slots in the
+// cell, so the cell ends up sorted by slot index whatever order the scatter's
+// atomics produced. With reorder, every particle is also copied to the slot
+// it takes in cell order (lennard_jones.wgsl:419-433).
+constexpr int kSortRegs = 8;  // cells up to 256 particles rank in registers
+
+__device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, uint32_t to,
+                                                uint32_t cell) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        a.sx[k * a.seg + to] = a.x[k * a.seg + from];
+        a.sv[k * a.seg + to] = a.v[k * a.seg + from];
+    }
+    a.sid[to] = a.id[from];
+    a.scell[to] = cell;
+}
+
+__global__ void sort_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cell >= a.ncells) return;
+    uint32_t b = box_of_cell(a, cell);
+    if (!rebuilding(a, b)) return;
+    const bool reorder = a.ctrl[b].reorder != 0u;
+    const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
+    const uint32_t m = end - start;
+    if (lane == 0) a.count[cell] = 0u;
+    if (m <= 32u * kSortRegs) {
+        uint32_t key[kSortRegs], rank[kSortRegs];
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
+            rank[r] = 0;
+        }
+        for (int rr = 0; rr < kSortRegs; rr++) {
+            if ((uint32_t)rr * 32u >= m) break;
+            for (int src = 0; src < 32; src++) {
+                uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
+#pragma unroll
+                for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            if (t < m) {
+                a.sorted[start + rank[r]] = key[r];
+                if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
+            }
+        }
+    } else if (lane == 0) {
+        // insertion sort, as the reference, for improbably full cells
+        for (uint32_t s = start + 1; s < end; s++) {
+            uint32_t key = a.sorted[s];
+            uint32_t t = s;
+            while (t > start && a.sorted[t - 1] > key) {
+                a.sorted[t] = a.sorted[t - 1];
+                t -= 1;
+            }
+            a.sorted[t] = key;
+        }
+        if (reorder)
+            for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
+    }
+}
+
+// ---- reorder copy back (lennard_jones.wgsl:435-452) ----
+__global__ void reorder_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nslots) return;
+    uint32_t b = box_of_slot(a, s);
+    if (!rebuilding(a, b) || !a.ctrl[b].reorder) return;
+    const Box& bx = a.boxes[b];
+    uint4 w;
+    double xs[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        xs[k] = a.sx[k * a.seg + s];
+        a.x[k * a.seg + s] = xs[k];
+        a.v[k * a.seg + s] = a.sv[k * a.seg + s];
+    }
+    a.id[s] = a.sid[s];
+    a.cell_of_slot[s] = a.scell[s];
+    a.sorted[s] = s;
+    w.x = encode(xs[0], bx.enc[0]);
+    w.y = encode(xs[1], bx.enc[1]);
+    w.z = encode(xs[2], bx.enc[2]);
+    w.w = 0u;
+    a.cache[a.glob->phase][s] = w;
+}
+
+// ---- the reference's packed positions for the list build
+// (lennard_jones.wgsl:154-164; hi/lo as Df64::from_f64, lennard_jones.rs:476-489)
+__global__ void pack_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nslots) return;
+    if (!rebuilding(a, box_of_slot(a, s))) return;
+    float h[3], l[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double x = a.x[k * a.seg + s];
+        h[k] = (float)x;
+        l[k] = (float)(x - (double)h[k]);
+    }
+    float3 hi = make_float3(h[0], h[1], h[2]);
+    float3 lo = make_float3(l[0], l[1], l[2]);
+    a.ref[s] = make_float4(h[0], h[1], h[2], __uint_as_float(pack_lo(hi, lo)));
+    a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
+}
+
+// ---- Verlet list build (lennard_jones.wgsl:454-499) ----
+// Everything within cutoff + skin, cells in the order dz, dy, dx = -1..1 with
+// periodic wrap, then each cell in sorted order; the distance test is the
+// reference's f32 arithmetic on packed positions, operation for operation.
+__global__ void build_list_kernel(Arena a) {
+    if (!a.glob->any) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    uint32_t b = box_of_slot(a, i);
+    if (!rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    const float4 own = a.ref[i];
+    const float4 own_lo = a.ref_lo[i];
+    const float xh[3] = {own.x, own.y, own.z};
+    const float xl[3] = {own_lo.x, own_lo.y, own_lo.z};
+    const int32_t nx = (int32_t)bx.cells[0], ny = (int32_t)bx.cells[1], nz = (int32_t)bx.cells[2];
+    const int32_t ci = (int32_t)(a.cell_of_slot[i] - bx.cell_base);
+    const int32_t cx = ci % nx, cy = (ci / nx) % ny, cz = ci / (nx * ny);
+    const uint32_t cap = bx.capacity;
+    const float list_r2 = bx.list_r2;
+    uint32_t found = 0;
+    for (int32_t dz = -1; dz <= 1; dz++)
+        for (int32_t dy = -1; dy <= 1; dy++)
+            for (int32_t dx = -1; dx <= 1; dx++) {
+                uint32_t ux = (uint32_t)((cx + dx + nx) % nx);
+                uint32_t uy = (uint32_t)((cy + dy + ny) % ny);
+                uint32_t uz = (uint32_t)((cz + dz + nz) % nz);
+                uint32_t cell = bx.cell_base + (uz * (uint32_t)ny + uy) * (uint32_t)nx + ux;
+                uint32_t end = a.cell_start[cell + 1];
+                for (uint32_t t = a.cell_start[cell]; t < end; t++) {
+                    uint32_t j = a.sorted[t];
+                    if (j == i) continue;
+                    float4 pj = a.ref[j];
+                    uint32_t bits = __float_as_uint(pj.w);
+                    float d0 = nearest_ref(__fadd_rn(__fsub_rn(pj.x, xh[0]),
+                                                     __fsub_rn(unpack_lo1(pj.x, bits, 0), xl[0])),
+                                           bx.box_f[0]);
+                    float d1 = nearest_ref(__fadd_rn(__fsub_rn(pj.y, xh[1]),
+                                                     __fsub_rn(unpack_lo1(pj.y, bits, 1), xl[1])),
+                                           bx.box_f[1]);
+                    float d2 = nearest_ref(__fadd_rn(__fsub_rn(pj.z, xh[2]),
+                                                     __fsub_rn(unpack_lo1(pj.z, bits, 2), xl[2])),
+                                           bx.box_f[2]);
+                    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)),
+                                         __fmul_rn(d2, d2));
+                    if (r2 < list_r2) {
+                        if (found < cap) a.list[(size_t)found * a.seg + i] = j;
+                        found += 1;
+                    }
+                }
+            }
+    a.list_count[i] = found < cap ? found : cap;
+    if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
+    a.snap[i] = a.cache[a.glob->phase][i];
+}
+
+// ---- forces from the list (lennard_jones.wgsl:503-530) ----
+// Separations come from the 32-bit box fractions: the wrapped integer
+// difference is the nearest image.
+template <bool SHIFTED_FORCE, bool ENERGIES>
+__device__ __forceinline__ void pair_sums(const Arena& a, const Box& bx, uint32_t i,
+                                          const uint4* __restrict__ cur, float& ax, float& ay,
+                                          float& az, float& pe, float& w, uint32_t& near) {
+    const uint4 own = __ldg(cur + i);
+    const uint32_t cnt = __ldg(a.list_count + i);
+    const uint32_t* __restrict__ row = a.list + i;
+    const size_t seg = a.seg;
+    const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
+    ax = ay = az = 0.0f;
+    pe = w = 0.0f;
+    near = 0;
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t j = __ldg(row + k * seg);
+        const uint4 pj = __ldg(cur + j);
+        const float dx = decode_diff(pj.x, own.x, dec0);
+        const float dy = decode_diff(pj.y, own.y, dec1);
+        const float dz = decode_diff(pj.z, own.z, dec2);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < rc2) {
+            float f;
+            if (ENERGIES) {
+                float rf, u;
+                lj_pair<SHIFTED_FORCE>(r2, bx, rf, u);
+                f = rf / r2;
+                pe += 0.5f * u;
+                w += 0.5f * rf;
+                near += r2 < 2.25f ? 1u : 0u;
+            } else {
+                f = lj_force_over_r2<SHIFTED_FORCE>(r2, bx);
+            }
+            ax -= dx * f;
+            ay -= dy * f;
+            az -= dz * f;
+        }
+    }
+}
+
+__device__ __forceinline__ double wrap(double x, double side) {
+    if (x >= side) x -= side;
+    if (x < 0.0) x += side;
+    if (x >= side) x -= side;
+    return x;
+}
+
+// ---- prime (lennard_jones.wgsl:547-553): first forces; the stored velocity
+// becomes half a kick behind the given one ----
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) prime_kernel(Arena a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[box_of_slot(a, i)];
+    const uint4* cur = a.cache[a.glob->phase];
+    float ax, ay, az, pe, w;
+    uint32_t near;
+    pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, w, near);
+    a.v[i] -= (double)ax * bx.half_dt;
+    a.v[a.seg + i] -= (double)ay * bx.half_dt;
+    a.v[2 * a.seg + i] -= (double)az * bx.half_dt;
+}
+
+// ---- one step: begin + force_kick of the reference fused
+// (lennard_jones.wgsl:204-276, 556-574) ----
+// The stored velocity is half a kick behind, so this kernel's force pass
+// applies the previous step's closing half kick and this step's opening half
+// kick together, then drifts: x += v dt (constant energy), or the Langevin
+// A-O-A: x += v dt/2; v = c1 v + c2 xi; x += v dt/2, with xi from the
+// Philox stream keyed by (seed, step, particle id). All state updates in f64.
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) step_kernel(Arena a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < a.nslots;
+    const uint32_t phase = a.glob->phase;
+    const uint4* cur = a.cache[phase];
+    uint4* nxt = a.cache[phase ^ 1u];
+    uint32_t b = 0;
+    float disp2 = 0.0f;
+    if (valid) {
+        b = box_of_slot(a, i);
+        const Box& bx = a.boxes[b];
+        float ax, ay, az, pe, w;
+        uint32_t near;
+        pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, w, near);
+        const float acc[3] = {ax, ay, az};
+        float3 xi = make_float3(0.0f, 0.0f, 0.0f);
+        const bool langevin = bx.thermostat == 1;
+        if (langevin) xi = langevin_noise(a.id[i], a.glob->step, bx.seed);
+        const float noise[3] = {xi.x, xi.y, xi.z};
+        uint32_t enc[3];
+        const uint4 snap = a.snap[i];
+        const uint32_t sw[3] = {snap.x, snap.y, snap.z};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            double x = a.x[k * a.seg + i];
+            double v = a.v[k * a.seg + i] + (double)acc[k] * bx.dt;
+            if (langevin) {
+                x += v * bx.half_dt;
+                v = bx.c1 * v + bx.c2 * (double)noise[k];
+                x += v * bx.half_dt;
+            } else {
+                x += v * bx.dt;
+            }
+            x = wrap(x, bx.box[k]);
+            a.x[k * a.seg + i] = x;
+            a.v[k * a.seg + i] = v;
+            enc[k] = encode(x, bx.enc[k]);
+            float d = decode_diff(enc[k], sw[k], bx.dec[k]);
+            disp2 += d * d;
+        }
+        nxt[i] = make_uint4(enc[0], enc[1], enc[2], 0u);
+    }
+    block_max_per_box(a, valid, b, disp2);
+    if (i == 0) a.glob->pending = 1u;
+}
+
+// ---- measure (lennard_jones.wgsl:576-626) ----
+// Per particle: half of each pair energy and virial (f32 sums over the list),
+// neighbours within 1.5 sigma, the velocity at the step (stored velocity plus
+// the closing half kick), kinetic energy and momentum in f64. Each value goes
+// to 32.32 fixed point scaled like the reference and is summed exactly.
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, int canonical) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < a.nslots;
+    uint32_t b = 0;
+    long long v[kSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (valid) {
+        b = box_of_slot(a, i);
+        const Box& bx = a.boxes[b];
+        const uint4* cur = a.cache[a.glob->phase];
+        float ax, ay, az, pe, w;
+        uint32_t near;
+        pair_sums<SHIFTED_FORCE, true>(a, bx, i, cur, ax, ay, az, pe, w, near);
+        const float acc[3] = {ax, ay, az};
+        double vel[3], ke = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            vel[k] = a.v[k * a.seg + i] + (double)acc[k] * bx.half_dt;
+            ke += vel[k] * vel[k];
+        }
+        ke *= 0.5;
+        const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
+        v[0] = fixed_raw_f64(ke * es);
+        v[1] = fixed_raw_f32(pe * bx.energy_scale);
+        v[2] = fixed_raw_f32(w * bx.energy_scale);
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[3 + k] = fixed_raw_f64(vel[k] * ms);
+        v[6] = near >= bx.near_count ? (1ll << 32) : 0ll;
+        a.pe_half[i] = pe;
+        a.w_half[i] = w;
+        a.vel4[i] = make_float4((float)vel[0], (float)vel[1], (float)vel[2], (float)near);
+        if (canonical) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) a.vcanon[k * a.seg + i] = vel[k];
+        }
+    }
+    block_sum_slots(a, valid, b, v);
+}
+
+// ---- launchers ----
+cudaError_t launch_encode(const Arena& a, cudaStream_t s) {
+    encode_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle) {
+    if (cond_handle)
+        decide_kernel<true><<<1, kBlock, 0, s>>>(a, (cudaGraphConditionalHandle)cond_handle);
+    else
+        decide_kernel<false><<<1, kBlock, 0, s>>>(a, (cudaGraphConditionalHandle)0);
+    return after_launch();
+}
+
+cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
+    const unsigned slots = blocks_for(a.nslots);
+    bin_kernel<<<slots, kBlock, 0, s>>>(a);
+    scan_kernel<<<a.nboxes, kScanThreads, 0, s>>>(a);
+    scatter_kernel<<<slots, kBlock, 0, s>>>(a);
+    sort_kernel<<<blocks_for(a.ncells * 32u), kBlock, 0, s>>>(a);
+    reorder_kernel<<<slots, kBlock, 0, s>>>(a);
+    pack_kernel<<<slots, kBlock, 0, s>>>(a);
+    build_list_kernel<<<slots, kBlock, 0, s>>>(a);
+    return after_launch(7);
+}
+
+cudaError_t launch_prime(const Arena& a, bool shifted_force, cudaStream_t s) {
+    if (shifted_force)
+        prime_kernel<true><<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    else
+        prime_kernel<false><<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_step(const Arena& a, bool shifted_force, cudaStream_t s) {
+    if (shifted_force)
+        step_kernel<true><<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    else
+        step_kernel<false><<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_measure(const Arena& a, bool shifted_force, bool canonical, cudaStream_t s) {
+    if (shifted_force)
+        measure_kernel<true><<<blocks_for(a.nslots), kBlock, 0, s>>>(a, canonical ? 1 : 0);
+    else
+        measure_kernel<false><<<blocks_for(a.nslots), kBlock, 0, s>>>(a, canonical ? 1 : 0);
+    return after_launch();
+}
+
+}  // namespace vlj

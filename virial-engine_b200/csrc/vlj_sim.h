@@ -1,0 +1,60 @@
+// The simulation object behind the opaque vlj_sim handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "virial_lj.h"
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+constexpr int kRing = 3;  // measurement read-back slots (lennard_jones.rs:320)
+
+// One measurement's words as read back into pinned host memory.
+struct Readback {
+    long long slots[kSlots];
+    Control ctrl;
+};
+
+double scale_for(double magnitude);
+vlj_status check_settings(const vlj_settings* st);
+vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3], double cutoff,
+                    double skin, double dt, bool shifted_force, const vlj_thermostat& t,
+                    uint32_t profile_bins, Box& b);
+
+}  // namespace vlj
+
+struct vlj_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    vlj_settings settings{};
+    uint32_t n = 0;
+    bool shifted_force = false;
+    vlj::Box box{};
+    vlj::Arena arena{};
+    std::vector<void*> allocations;
+    uint64_t steps = 0;
+    // measurement read-back ring
+    vlj::Readback* ring = nullptr;
+    cudaEvent_t ring_event[vlj::kRing] = {};
+    bool ring_busy[vlj::kRing] = {};
+    uint64_t ring_step[vlj::kRing] = {};
+    // profiles
+    uint64_t profile_samples = 0;
+    // heat current series
+    uint32_t series_samples = 0;
+    // captured steps
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_graph_exec = nullptr;
+    uint32_t graph_steps = 0;
+
+    ~vlj_sim();
+};
+
+namespace vlj {
+vlj_status sim_allocate(vlj_sim* s, void* stream);
+vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
+}  // namespace vlj

@@ -1,0 +1,516 @@
+"""Python mirror of virial_particles::lennard_jones over the B200 CUDA library.
+
+Same names and argument meanings as the reference's Rust API
+(crates/virial-particles/src/lennard_jones.rs): `LennardJones(particles,
+settings)`, `step`, `run`, `measure`/`poll`/`measure_now`, `read_particles`,
+profiles along z, the heat current, setters, and the `lattice` helpers.
+The reference panics on misuse; here every failure raises `VljError` carrying
+the C ABI status. Particles are numpy arrays of dtype `PARTICLE`
+(fields `pos` and `vel`, three f64 each), the layout of `vlj_particle`.
+
+All work runs in the CUDA library (libvirial_lj.so); there is no CPU path:
+importing this module without the built library raises ImportError.
+"""
+
+import ctypes as C
+import enum
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import PARTICLE
+
+_lib = _ffi.load()
+
+__all__ = [
+    "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
+    "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
+    "lattice_fcc", "particles", "device_count", "library_path", "launches",
+]
+
+
+class VljError(RuntimeError):
+    """A C ABI call failed; `status` is the vlj_status name."""
+
+    def __init__(self, status, message):
+        self.status = _ffi.STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.status}: {message}")
+
+
+def _check(status):
+    if status != 0:
+        raise VljError(status, _lib.vlj_last_error().decode(errors="replace"))
+
+
+def library_path():
+    return _ffi.LIB_PATH
+
+
+def device_count():
+    n = C.c_int()
+    _check(_lib.vlj_device_count(C.byref(n)))
+    return n.value
+
+
+def launches():
+    """Kernel launches this library has made in this process."""
+    n = C.c_uint64()
+    _check(_lib.vlj_debug_launches(C.byref(n)))
+    return n.value
+
+
+def particles(pos, vel=None):
+    """Particle array from n x 3 positions (and velocities)."""
+    pos = np.asarray(pos, dtype=np.float64)
+    out = np.zeros(len(pos), PARTICLE)
+    out["pos"] = pos
+    if vel is not None:
+        out["vel"] = np.asarray(vel, dtype=np.float64)
+    return out
+
+
+# ---- settings (lennard_jones.rs:32-82) ----
+
+@dataclass
+class Langevin:
+    temperature: float
+    friction: float
+    seed: int
+
+
+@dataclass
+class NoseHoover:
+    temperature: float
+    period: float
+
+
+Thermostat = Optional[Union[Langevin, NoseHoover]]
+
+
+@dataclass
+class Settings:
+    box_size: Sequence[float]
+    cutoff: float = 2.5
+    dt: float = 0.005
+    thermostat: Thermostat = None
+    shifted_force: bool = False
+    skin: float = 0.3
+    profile_bins: int = 0
+
+    def _c(self):
+        t = _ffi.Thermostat()
+        if isinstance(self.thermostat, Langevin):
+            t.kind, t.temperature, t.friction, t.seed = 1, self.thermostat.temperature, \
+                self.thermostat.friction, self.thermostat.seed & 0xFFFFFFFF
+        elif isinstance(self.thermostat, NoseHoover):
+            t.kind, t.temperature, t.period = 2, self.thermostat.temperature, self.thermostat.period
+        elif self.thermostat is not None:
+            raise TypeError("thermostat must be None, Langevin or NoseHoover")
+        s = _ffi.Settings()
+        s.box_size[:] = [float(x) for x in self.box_size]
+        s.cutoff, s.dt, s.thermostat = self.cutoff, self.dt, t
+        s.shifted_force, s.skin, s.profile_bins = int(bool(self.shifted_force)), self.skin, \
+            self.profile_bins
+        return s
+
+
+# ---- results (lennard_jones.rs:84-280) ----
+
+@dataclass
+class Measurement:
+    step: int
+    time: float
+    kinetic: float
+    potential: float
+    virial: float
+    momentum: List[float]
+    count: int
+    volume: float
+    list_rebuilds: int
+    list_overflow: int
+    thermostat_energy: float
+    condensed: int
+
+    @staticmethod
+    def _from(m):
+        return Measurement(m.step, m.time, m.kinetic, m.potential, m.virial, list(m.momentum),
+                           m.count, m.volume, m.list_rebuilds, m.list_overflow,
+                           m.thermostat_energy, m.condensed)
+
+    def energy(self):
+        return self.kinetic + self.potential
+
+    def temperature(self, dof):
+        """2 KE / dof: 3N with a thermostat, 3N - 3 at constant energy."""
+        return 2.0 * self.kinetic / dof
+
+    def pressure(self):
+        """P = (2 KE + W) / (3 V), the virial theorem."""
+        return (2.0 * self.kinetic + self.virial) / (3.0 * self.volume)
+
+    def extended_energy(self):
+        return self.energy() + self.thermostat_energy
+
+
+@dataclass
+class Slab:
+    z: float
+    particles: float
+    kinetic: List[float]
+    virial: List[float]
+    potential: float
+
+
+class Phase(enum.IntEnum):
+    LIQUID = 0
+    VAPOUR = 1
+    INTERFACE = 2
+    BETWEEN = 3
+
+
+class Drawn(enum.IntEnum):
+    NEIGHBOURS = 0
+    TEMPERATURE = 1
+
+
+@dataclass
+class Profile:
+    samples: int
+    box_size: List[float]
+    slabs: List[Slab]
+    virial: List[float] = field(default_factory=lambda: [0.0, 0.0, 0.0])
+
+    def slab_volume(self):
+        lx, ly, lz = self.box_size
+        return lx * ly * lz / len(self.slabs)
+
+    def density(self):
+        v = self.slab_volume()
+        return [s.particles / v for s in self.slabs]
+
+    def temperature(self):
+        return [sum(s.kinetic) / (3.0 * s.particles) if s.particles else math.nan
+                for s in self.slabs]
+
+    def pressure_tensor(self):
+        v = self.slab_volume()
+        return [[(s.kinetic[a] + s.virial[a]) / v for a in range(3)] for s in self.slabs]
+
+    def total_pressure_tensor(self):
+        volume = self.box_size[0] * self.box_size[1] * self.box_size[2]
+        return [(sum(s.kinetic[a] for s in self.slabs) + self.virial[a]) / volume
+                for a in range(3)]
+
+    def interfaces(self, midpoint):
+        d = np.ascontiguousarray(self.density(), np.float64)
+        found = C.c_size_t()
+        out = np.zeros(len(d), np.float64)
+        _check(_lib.vlj_profile_interfaces(d.ctypes.data_as(C.POINTER(C.c_double)), len(d),
+                                           float(self.box_size[2]), midpoint,
+                                           out.ctypes.data_as(C.POINTER(C.c_double)), len(out),
+                                           C.byref(found)))
+        return list(out[:found.value])
+
+    def phases(self, midpoint, margin):
+        d = np.ascontiguousarray(self.density(), np.float64)
+        out = np.zeros(len(d), np.int32)
+        _check(_lib.vlj_profile_phases(d.ctypes.data_as(C.POINTER(C.c_double)), len(d),
+                                       float(self.box_size[2]), midpoint, margin,
+                                       out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return [Phase(int(p)) for p in out]
+
+    def mean_in(self, values, phases, phase):
+        chosen = [v for v, p in zip(values, phases) if p == phase]
+        return sum(chosen) / len(chosen) if chosen else None
+
+    def surface_tension(self):
+        pxx, pyy, pzz = self.total_pressure_tensor()
+        return 0.5 * self.box_size[2] * (pzz - 0.5 * (pxx + pyy))
+
+
+@dataclass
+class HeatExchange:
+    hot: Sequence[float]
+    cold: Sequence[float]
+    energy: float
+
+
+# ---- the simulation (lennard_jones.rs:334-1375) ----
+
+class LennardJones:
+    """Lennard-Jones particles in a periodic box on one GPU."""
+
+    def __init__(self, particles, settings: Settings, stream=None):
+        p = np.ascontiguousarray(particles, dtype=PARTICLE)
+        self._settings = settings
+        h = C.c_void_p()
+        cs = settings._c()
+        _check(_lib.vlj_create(_ffi.ptr(p), len(p), C.byref(cs), stream, C.byref(h)))
+        self._h = h
+        self._n = len(p)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.vlj_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # accessors
+    def count(self):
+        return self._n
+
+    def box_size(self):
+        out = (C.c_double * 3)()
+        _check(_lib.vlj_box_size(self._h, out))
+        return list(out)
+
+    def volume(self):
+        v = C.c_double()
+        _check(_lib.vlj_volume(self._h, C.byref(v)))
+        return v.value
+
+    def steps(self):
+        v = C.c_uint64()
+        _check(_lib.vlj_steps(self._h, C.byref(v)))
+        return v.value
+
+    def time(self):
+        v = C.c_double()
+        _check(_lib.vlj_time(self._h, C.byref(v)))
+        return v.value
+
+    def target_temperature(self):
+        has, t = C.c_int(), C.c_double()
+        _check(_lib.vlj_target_temperature(self._h, C.byref(has), C.byref(t)))
+        return t.value if has.value else None
+
+    def positions(self):
+        """(device pointer, stride): three f64 arrays x, y, z of `stride` each."""
+        p, stride = C.c_void_p(), C.c_size_t()
+        _check(_lib.vlj_positions(self._h, C.byref(p), C.byref(stride)))
+        return p.value, stride.value
+
+    def velocities(self):
+        """Device pointer to float4 (vx, vy, vz, drawn) per slot."""
+        p = C.c_void_p()
+        _check(_lib.vlj_velocities(self._h, C.byref(p)))
+        return p.value
+
+    # stepping
+    def step(self, steps=1):
+        _check(_lib.vlj_step(self._h, int(steps)))
+
+    def run(self, steps):
+        _check(_lib.vlj_run(self._h, int(steps)))
+
+    # measurements
+    def measure(self):
+        ok = C.c_int()
+        _check(_lib.vlj_measure(self._h, C.byref(ok)))
+        return bool(ok.value)
+
+    def after_submit(self):
+        """Nothing to do: work goes to the stream when it is enqueued."""
+
+    def poll(self):
+        buf = (_ffi.Measurement * 8)()
+        n = C.c_size_t()
+        _check(_lib.vlj_poll(self._h, buf, 8, C.byref(n)))
+        return [Measurement._from(buf[i]) for i in range(n.value)]
+
+    def measure_now(self):
+        m = _ffi.Measurement()
+        _check(_lib.vlj_measure_now(self._h, C.byref(m)))
+        return Measurement._from(m)
+
+    # state
+    def read_particles(self):
+        out = np.zeros(self._n, PARTICLE)
+        _check(_lib.vlj_read_particles(self._h, _ffi.ptr(out)))
+        return out
+
+    def write_particles(self, particles):
+        p = np.ascontiguousarray(particles, dtype=PARTICLE)
+        _check(_lib.vlj_write_particles(self._h, _ffi.ptr(p), len(p)))
+
+    # setters
+    def set_drawn(self, drawn: Drawn):
+        _check(_lib.vlj_set_drawn(self._h, int(drawn)))
+
+    def set_condensed_neighbours(self, neighbours):
+        _check(_lib.vlj_set_condensed_neighbours(self._h, int(neighbours)))
+
+    def set_temperature(self, temperature):
+        _check(_lib.vlj_set_temperature(self._h, float(temperature)))
+
+    def set_heat_exchange(self, exchange: Optional[HeatExchange]):
+        if exchange is None:
+            _check(_lib.vlj_set_heat_exchange(self._h, None))
+            return
+        h = _ffi.HeatExchange()
+        h.hot[:] = list(exchange.hot)
+        h.cold[:] = list(exchange.cold)
+        h.energy = exchange.energy
+        _check(_lib.vlj_set_heat_exchange(self._h, C.byref(h)))
+
+    def heat_flux(self):
+        has, f = C.c_int(), C.c_double()
+        _check(_lib.vlj_heat_flux(self._h, C.byref(has), C.byref(f)))
+        return f.value if has.value else None
+
+    # profiles
+    def sample_profile(self):
+        _check(_lib.vlj_sample_profile(self._h))
+
+    def sample_profile_now(self):
+        self.sample_profile()
+
+    def clear_profile(self):
+        _check(_lib.vlj_clear_profile(self._h))
+
+    def read_profile(self):
+        bins = self._settings.profile_bins
+        slabs = (_ffi.Slab * max(bins, 1))()
+        virial = (C.c_double * 3)()
+        samples = C.c_uint64()
+        _check(_lib.vlj_read_profile(self._h, slabs, virial, C.byref(samples)))
+        out = [Slab(s.z, s.particles, list(s.kinetic), list(s.virial), s.potential)
+               for s in slabs[:bins]]
+        return Profile(samples.value, self.box_size(), out, list(virial))
+
+    # heat current
+    def record_heat_current(self, capacity):
+        self._series_capacity = int(capacity)
+        _check(_lib.vlj_record_heat_current(self._h, int(capacity)))
+
+    def sample_heat_current(self):
+        _check(_lib.vlj_sample_heat_current(self._h))
+
+    def read_heat_current(self):
+        cap = getattr(self, "_series_capacity", 0)
+        out = np.zeros((max(cap, 1), 3))
+        n = C.c_size_t()
+        _check(_lib.vlj_read_heat_current(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                          cap, C.byref(n)))
+        return out[:n.value].copy()
+
+    # inspection for tests
+    def grid_info(self):
+        g = _ffi.GridInfo()
+        _check(_lib.vlj_debug_grid_info(self._h, C.byref(g)))
+        return g
+
+    def read_grid(self):
+        g = self.grid_info()
+        n = self._n
+        out = dict(
+            sorted=np.zeros(n, np.uint32), cell_start=np.zeros(g.total_cells + 1, np.uint32),
+            cell_of_slot=np.zeros(n, np.uint32), ids=np.zeros(n, np.uint32),
+            counts=np.zeros(n, np.uint32), lists=np.zeros((n, g.capacity), np.uint32),
+            x=np.zeros((n, 3)), v=np.zeros((n, 3)))
+        _check(_lib.vlj_debug_read_grid(
+            self._h, *[_ffi.ptr(out[k]) for k in
+                       ("sorted", "cell_start", "cell_of_slot", "ids", "counts", "lists", "x", "v")]))
+        return out
+
+    def force_rebuild(self):
+        _check(_lib.vlj_debug_force_rebuild(self._h))
+
+    def read_partials(self):
+        pe = np.zeros(self._n, np.float32)
+        w = np.zeros(self._n, np.float32)
+        raw = np.zeros(8, np.int64)
+        _check(_lib.vlj_debug_read_partials(self._h, _ffi.ptr(pe), _ffi.ptr(w), _ffi.ptr(raw)))
+        return pe, w, raw
+
+
+# ---- batched replicas (no reference counterpart) ----
+
+@dataclass
+class Replica:
+    particles: np.ndarray
+    box_size: Sequence[float]
+    thermostat: Thermostat = None
+
+
+class Batch:
+    """Many independent periodic boxes stepped together in one launch per step."""
+
+    def __init__(self, replicas: Sequence[Replica], cutoff=2.5, skin=0.3, dt=0.005,
+                 shifted_force=False, stream=None):
+        self._keep = [np.ascontiguousarray(r.particles, dtype=PARTICLE) for r in replicas]
+        descs = (_ffi.ReplicaDesc * len(replicas))()
+        for d, r, p in zip(descs, replicas, self._keep):
+            d.particles = p.ctypes.data
+            d.count = len(p)
+            d.box_size[:] = [float(x) for x in r.box_size]
+            d.thermostat = Settings(r.box_size, thermostat=r.thermostat)._c().thermostat
+        h = C.c_void_p()
+        _check(_lib.vlj_batch_create(descs, len(replicas), cutoff, skin, dt, int(shifted_force),
+                                     stream, C.byref(h)))
+        self._h = h
+        self._counts = [len(p) for p in self._keep]
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.vlj_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def replicas(self):
+        return len(self._counts)
+
+    def total(self):
+        return sum(self._counts)
+
+    def step(self, steps=1):
+        _check(_lib.vlj_batch_step(self._h, int(steps)))
+
+    def measure(self):
+        buf = (_ffi.Measurement * len(self._counts))()
+        _check(_lib.vlj_batch_measure(self._h, buf))
+        return [Measurement._from(m) for m in buf]
+
+    def read_particles(self, replica):
+        out = np.zeros(self._counts[replica], PARTICLE)
+        _check(_lib.vlj_batch_read_particles(self._h, int(replica), _ffi.ptr(out)))
+        return out
+
+
+# ---- host helpers (lennard_jones.rs:1377-1441) ----
+
+def lattice(count, box_size, temperature, seed):
+    out = np.zeros(int(count), PARTICLE)
+    _check(_lib.vlj_lattice(int(count), float(box_size), float(temperature), int(seed),
+                            _ffi.ptr(out)))
+    return out
+
+
+def lattice_box(count, size, temperature, seed):
+    out = np.zeros(int(count), PARTICLE)
+    sz = (C.c_double * 3)(*[float(s) for s in size])
+    _check(_lib.vlj_lattice_box(int(count), sz, float(temperature), int(seed), _ffi.ptr(out)))
+    return out
+
+
+def lattice_fcc(cells, density, temperature, seed):
+    """fcc lattice of cells^3 unit cells; returns (particles, box side)."""
+    out = np.zeros(4 * int(cells) ** 3, PARTICLE)
+    box = C.c_double()
+    _check(_lib.vlj_lattice_fcc(int(cells), float(density), float(temperature), int(seed),
+                                _ffi.ptr(out), C.byref(box)))
+    return out, box.value
