@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Lennard-Jones particle-steps/s on B200.
+
+Workload (default): 256,000 atoms on an fcc lattice (40^3 unit cells x 4) at
+rho = 0.8442, force-shifted cutoff 2.5, Langevin T = 1.0, gamma = 1.0, seed 7,
+dt = 0.005, Verlet list with skin 0.3 rebuilt on the skin/2 trigger (cell grid
+rebuilt with it), f32 pair forces, i64 fixed-point energy and virial, f64
+integration. Synthetic seeded input, no dataset.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One timed step is one MD step of the whole box. Between timed steps a
+256 MiB buffer is written on the same stream to flush the 126 MB L2, so every
+step starts cold; each step is bracketed by CUDA events on the simulation's
+stream and the per-step device times are summed. Under torchrun every rank
+runs its own independent box (weak scaling, no collective on the step path);
+the time is the max over ranks.
+
+`e2e`: the same metric through the public API with host buffers: per bench
+step, the particles are written from host memory (vlj_write_particles),
+100 MD steps run (vlj_run), and the measurement and the particles are read
+back (vlj_measure_now, vlj_read_particles); wall clock, max over ranks.
+
+`--impl reference`: the reference has no CPU Lennard-Jones code and its GPU
+path needs a graphics API, so the reference arm is the CPU oracle's f64
+cell-list engine (same model, integrator and workload) on all host cores,
+rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "virial-engine_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "LJ particle-steps/s on 1 B200, batched vs plain, at <=1e-6 rel PE/virial vs f64"
+UNIT = "particle-steps/s"
+WORK = dict(cells=40, density=0.8442, temperature=1.0, friction=1.0, seed=7, dt=0.005,
+            cutoff=2.5, skin=0.3, shifted_force=True)
+E2E_INNER = 100          # MD steps per end-to-end bench step
+L2_FLUSH_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
+ALGO_BYTES = 96          # f64 x and v read + written per particle-step
+
+
+def config(n, world):
+    return {
+        "workload": "lj-fcc40x4-256k-rho0.8442-shifted-force-langevin",
+        "particles_per_box": n, "boxes": world, "density": WORK["density"],
+        "cutoff": WORK["cutoff"], "cutoff_style": "force-shifted", "skin": WORK["skin"],
+        "thermostat": "langevin T=1.0 gamma=1.0 seed=7", "dt": WORK["dt"],
+        "l2": "flushed between timed steps (256 MiB write on the stream)",
+        "parallelism": f"replicas x{world}",
+    }
+
+
+def flops_per_particle_step(density):
+    """Algorithmic f32 flops: 11 per list candidate, 26 per force-shifted pair
+    inside the cutoff (FMA = 2)."""
+    import math
+    n_list = 4.0 / 3.0 * math.pi * (WORK["cutoff"] + WORK["skin"]) ** 3 * density
+    n_rc = 4.0 / 3.0 * math.pi * WORK["cutoff"] ** 3 * density
+    return 11.0 * n_list + 26.0 * n_rc
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "step_kernel_lj256k.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    gpu_index = local
+    if world > 1:
+        # one GPU per process; the CUDA library and torch both see it as device 0
+        visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ids = visible.split(",") if visible else [str(i) for i in range(64)]
+        gpu_index = int(ids[local]) if ids[local].isdigit() else local
+        os.environ["CUDA_VISIBLE_DEVICES"] = ids[local]
+    return world, rank, gpu_index
+
+
+def reduce_max(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_port_rate(n_target_seconds, pos, vel, box, n_warm=2):
+    """The f64 oracle engine on this workload: (particle-steps/s, steps, cores)."""
+    import oracle as O
+    md = O.MD(pos, vel, [box] * 3, cutoff=WORK["cutoff"], skin=WORK["skin"], dt=WORK["dt"],
+              shifted_force=True, langevin=(WORK["temperature"], WORK["friction"], WORK["seed"]))
+    md.run(n_warm)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        md.run(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if (el >= n_target_seconds and steps >= 3) or steps >= 2000:
+            break
+    md.close()
+    return len(pos) * steps / el, steps, O.threads(), el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle as O
+    pos, vel, box = O.lattice_fcc(WORK["cells"], WORK["density"], WORK["temperature"], WORK["seed"])
+    n = len(pos)
+    md = O.MD(pos, vel, [box] * 3, cutoff=WORK["cutoff"], skin=WORK["skin"], dt=WORK["dt"],
+              shifted_force=True, langevin=(WORK["temperature"], WORK["friction"], WORK["seed"]))
+    md.run(args.warmup)
+    t0 = time.perf_counter()
+    md.run(args.steps)
+    el = time.perf_counter() - t0
+    md.close()
+    value = n * args.steps / el
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config(n, 1), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
+                         "sample": f"{args.steps} MD steps of the {n}-particle box after "
+                                   f"{args.warmup} warm-up steps (f64 OpenMP cell-list engine)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's LJ path runs only through wgpu (graphics API, unavailable on "
+                "this box) and its CPU crate has no LJ code; this arm is the oracle's f64 port",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, gpu_index):
+    import numpy as np
+    import torch
+    import virial_lj as vl
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    p, box = vl.lattice_fcc(WORK["cells"], WORK["density"], WORK["temperature"], WORK["seed"] + rank)
+    n = len(p)
+    settings = vl.Settings([box] * 3, cutoff=WORK["cutoff"], dt=WORK["dt"],
+                           thermostat=vl.Langevin(WORK["temperature"], WORK["friction"],
+                                                  WORK["seed"] + rank),
+                           shifted_force=True, skin=WORK["skin"])
+    sim = vl.LennardJones(p, settings, stream=stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+
+    # warm-up
+    sim.step(max(args.warmup, 3))
+    stream.synchronize()
+
+    # ---- timed region: K steps, L2 flushed between them ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    reb0 = sim.measure_now().list_rebuilds
+    k0 = sim.kernels_executed()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(gpu_index)
+    if rank == 0:
+        clocks.start()
+    for k in range(args.steps):
+        flush_l2()
+        starts[k].record(stream)
+        sim.step(1)
+        ends[k].record(stream)
+    stream.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = clocks.stop() if rank == 0 else None
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    launches = sim.kernels_executed() - k0  # this library's kernels that ran in the region
+    m = sim.measure_now()
+    rebuilds = m.list_rebuilds - reb0
+    max_ms = reduce_max(world, total_ms)
+    value = world * n * args.steps / (max_ms / 1e3)
+
+    # ---- the step kernel alone, for the roofline (CUDA events around each launch) ----
+    sim.kernel_timing(True)
+    for k in range(args.steps):
+        flush_l2()
+        sim.step(1)
+    kern_ms, kern_n = sim.kernel_time()
+    sim.kernel_timing(False)
+    avg_kernel_s = kern_ms / 1e3 / max(kern_n, 1)
+    peak, peak_kind = measured_peaks()
+    achieved = ALGO_BYTES * n / avg_kernel_s / 1e9
+    fp32_peak = vl.fp32_peak()
+    fpps = flops_per_particle_step(WORK["density"])
+    fp32_achieved = fpps * n / avg_kernel_s / 1e12
+    traffic = profile_traffic()
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e_steps = max(3, min(args.steps, 10))
+    host = vl.lattice_fcc(WORK["cells"], WORK["density"], WORK["temperature"], WORK["seed"] + rank)[0]
+    sim.write_particles(host)
+    sim.run(E2E_INNER)  # warm
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.write_particles(host)
+        sim.run(E2E_INNER)
+        meas = sim.measure_now()
+        back = sim.read_particles()
+    e2e_s = time.perf_counter() - t0
+    e2e_max = reduce_max(world, e2e_s)
+    e2e_value = world * n * E2E_INNER * e2e_steps / e2e_max
+    g = sim.grid_info()
+    seg = g.segment
+    h2d = seg * (24 + 24 + 4)
+    d2h = seg * (24 + 24 + 4) + 8 * 8 + 32
+
+    # ---- CPU baseline (rank 0, one GPU only) ----
+    cpu = None
+    if rank == 0 and world == 1:
+        rate, steps, cores, el = cpu_port_rate(args.cpu_seconds, p["pos"], p["vel"], box)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{steps} MD steps of the same {n}-particle box ({el:.1f} s, f64 "
+                         f"OpenMP cell-list engine, 2 warm-up steps)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "state_dtype": "f64",
+            "data": "synthetic", "config": config(n, world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": f"per bench step: write particles, {E2E_INNER} MD steps, "
+                            "measure_now, read_particles; wall clock"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "step_kernel<true>", "peak_source": peak_kind,
+                         "algorithmic_bytes_per_particle_step": ALGO_BYTES,
+                         "avg_kernel_us": avg_kernel_s * 1e6, "kernel_launches_timed": kern_n},
+            "fp32_roofline": {"achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                              "frac": fp32_achieved / fp32_peak if fp32_peak else None,
+                              "flops_per_particle_step": fpps,
+                              "peak_source": "measured live (FMA chains on every SM)"},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "list_rebuilds_timed": rebuilds,
+            "check": {"potential": meas.potential, "virial": meas.virial,
+                      "temperature": 2 * meas.kinetic / (3 * n), "list_overflow": meas.list_overflow},
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world, rank, gpu_index = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, gpu_index)
+
+
+if __name__ == "__main__":
+    main()

@@ -263,12 +263,26 @@ VLJ_API vlj_status vlj_debug_read_grid(vlj_sim *sim, uint32_t *sorted, uint32_t 
                                        double *vel_stored);
 /* Forces a list rebuild now (the decision ignores the displacement). */
 VLJ_API vlj_status vlj_debug_force_rebuild(vlj_sim *sim);
-/* Per-slot f32 halves of each particle's pair energy and virial from the
- * last measurement (n each), and the raw 64-bit fixed-point slots (8). */
+/* Per-slot halves of each particle's pair energy and virial from the last
+ * measurement, as (hi, lo) f32 pairs whose exact sum is the value (2n each),
+ * and the raw 64-bit fixed-point slots (8). */
 VLJ_API vlj_status vlj_debug_read_partials(vlj_sim *sim, float *pe_half, float *w_half,
                                            int64_t *raw_slots);
-/* Number of kernel launches this library made so far (all simulations). */
+/* Kernel launches this library enqueued from the host so far (all
+ * simulations; a graph launch counts its always-run nodes). */
 VLJ_API vlj_status vlj_debug_launches(uint64_t *launches);
+/* Kernels of this simulation that ran on the device (waits). */
+VLJ_API vlj_status vlj_debug_kernels_executed(vlj_sim *sim, uint64_t *kernels);
+/* 0: enqueue steps as direct launches instead of CUDA graphs. */
+VLJ_API vlj_status vlj_debug_set_graphs(vlj_sim *sim, int on);
+/* While on, steps are direct launches with CUDA events around every launch
+ * of the step kernel; vlj_debug_kernel_time returns their summed device time
+ * and count since timing was switched on or last read. */
+VLJ_API vlj_status vlj_debug_kernel_timing(vlj_sim *sim, int on);
+VLJ_API vlj_status vlj_debug_kernel_time(vlj_sim *sim, double *total_ms, uint64_t *launches);
+/* FP32 FMA throughput of the current device in TFLOP/s (a calibration kernel
+ * of independent FMA chains on every SM). */
+VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
 
 #ifdef __cplusplus
 }

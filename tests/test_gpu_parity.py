@@ -110,8 +110,8 @@ def test_fixed_point_totals_are_exact(gpu, O):
     pe, w, raw = sim.read_partials()
     es = O.setup(vel, [11.0] * 3, 2.5, 0.3, False).energy_scale
     to_raw = lambda a: int(np.rint(a.astype(np.float64) * es * 2.0 ** 32).astype(np.int64).sum())
-    assert raw[1] == to_raw(pe)
-    assert raw[2] == to_raw(w)
+    assert raw[1] == to_raw(pe[:, 0]) + to_raw(pe[:, 1])
+    assert raw[2] == to_raw(w[:, 0]) + to_raw(w[:, 1])
 
 
 def test_thermostatted_reruns_are_bit_identical(gpu):
@@ -235,3 +235,28 @@ def test_large_box_lists_and_energies(gpu, O, thermostat):
     assert rel(m.potential, pe) < TOL, (m.potential, pe)
     assert rel(m.virial, w.sum()) < TOL, (m.virial, w.sum())
     assert m.list_overflow == 0
+
+
+def test_graph_and_direct_launches_agree_bit_for_bit(gpu):
+    p, L = gpu.lattice_fcc(10, 0.8442, 1.0, 3)
+    st = gpu.Settings([L] * 3, dt=0.005, shifted_force=True, thermostat=gpu.Langevin(1.0, 1.0, 2))
+    out = []
+    for graphs in (True, False):
+        sim = gpu.LennardJones(p, st)
+        sim.set_graphs(graphs)
+        sim.run(137)  # chunks of 16 plus single steps
+        m = sim.measure_now()
+        out.append((sim.read_particles().tobytes(), m.potential, m.virial, m.list_rebuilds))
+    assert out[0] == out[1]
+
+
+def test_kernel_counter_counts_skipped_rebuilds_out(gpu):
+    p, L = gpu.lattice_fcc(10, 0.8442, 0.5, 3)
+    sim = gpu.LennardJones(p, gpu.Settings([L] * 3, dt=0.002))
+    sim.run(5)
+    r0, k0 = sim.measure_now().list_rebuilds, sim.kernels_executed()
+    sim.run(64)
+    k1 = sim.kernels_executed()
+    r1 = sim.measure_now().list_rebuilds
+    # two kernels per step plus seven per rebuild
+    assert k1 - k0 == 2 * 64 + 7 * (r1 - r0)

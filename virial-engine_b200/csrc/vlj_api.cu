@@ -108,6 +108,12 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
     b.rc2 = (float)rc2;
     b.list_r2 = (float)(list_radius * list_radius);
     b.half_skin2 = (float)(0.25 * skin * skin);
+    // The reference's f32 separations can be off by a few units in the last
+    // place of the box side for pairs across the boundary; widen past that.
+    double side_max = std::max(b.box[0], std::max(b.box[1], b.box[2]));
+    double pre_r = std::sqrt((double)b.list_r2) + 8.0 * std::ldexp(1.0, std::ilogb(side_max) - 23) + 1e-4;
+    b.prefilter_r2 = (float)(pre_r * pre_r);
+    for (int k = 0; k < 3; k++) b.inv_box_f[k] = 1.0f / b.box_f[k];
     b.dt = dt;
     b.half_dt = 0.5 * dt;
     b.c1 = 1.0;
@@ -164,8 +170,9 @@ double rem_euclid(double x, double side) {
 // uploads; ids are the input order.
 vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
     const size_t seg = s->arena.seg;
-    std::vector<double> x(3 * seg, 0.0), v(3 * seg, 0.0);
-    std::vector<uint32_t> id(seg, 0u);
+    double* x = s->pin_x;
+    double* v = s->pin_v;
+    uint32_t* id = s->pin_id;
     for (size_t i = 0; i < count; i++) {
         for (int k = 0; k < 3; k++) {
             if (!std::isfinite(p[i].pos[k]) || !std::isfinite(p[i].vel[k]))
@@ -175,12 +182,12 @@ vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
         }
         id[i] = (uint32_t)i;
     }
-    CUDA_TRY(cudaMemcpyAsync(s->arena.x, x.data(), sizeof(double) * 3 * seg,
-                             cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->arena.v, v.data(), sizeof(double) * 3 * seg,
-                             cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->arena.id, id.data(), sizeof(uint32_t) * seg,
-                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.x, x, sizeof(double) * 3 * seg, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.v, v, sizeof(double) * 3 * seg, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.id, id, sizeof(uint32_t) * seg, cudaMemcpyHostToDevice,
+                             s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return VLJ_OK;
 }
@@ -253,8 +260,14 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
 }  // namespace
 
 vlj_sim::~vlj_sim() {
-    if (step_graph_exec) cudaGraphExecDestroy(step_graph_exec);
-    if (step_graph) cudaGraphDestroy(step_graph);
+    if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
+    if (graph_one) cudaGraphExecDestroy(graph_one);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    for (cudaEvent_t e : ev_start) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_end) cudaEventDestroy(e);
+    if (pin_x) cudaFreeHost(pin_x);
+    if (pin_v) cudaFreeHost(pin_v);
+    if (pin_id) cudaFreeHost(pin_id);
     for (int k = 0; k < kRing; k++)
         if (ring_event[k]) cudaEventDestroy(ring_event[k]);
     if (ring) cudaFreeHost(ring);
@@ -392,14 +405,15 @@ vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
     if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
     TRY(enqueue_measure(s, true, -1));
     const size_t seg = s->arena.seg;
-    std::vector<double> x(3 * seg), v(3 * seg);
-    std::vector<uint32_t> id(seg);
-    CUDA_TRY(cudaMemcpyAsync(x.data(), s->arena.x, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
+    double* x = s->pin_x;
+    double* v = s->pin_v;
+    uint32_t* id = s->pin_id;
+    CUDA_TRY(cudaMemcpyAsync(x, s->arena.x, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
                              s->stream));
-    CUDA_TRY(cudaMemcpyAsync(v.data(), s->arena.vcanon, sizeof(double) * 3 * seg,
-                             cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(id.data(), s->arena.id, sizeof(uint32_t) * seg,
-                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(v, s->arena.vcanon, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(id, s->arena.id, sizeof(uint32_t) * seg, cudaMemcpyDeviceToHost,
+                             s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     for (uint32_t slot = 0; slot < s->n; slot++) {
         uint32_t i = id[slot];
@@ -581,11 +595,83 @@ vlj_status vlj_debug_read_partials(vlj_sim* s, float* pe_half, float* w_half, in
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (pe_half)
-        CUDA_TRY(cudaMemcpy(pe_half, s->arena.pe_half, sizeof(float) * s->n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(pe_half, s->arena.pe_half, sizeof(float) * 2 * s->n,
+                            cudaMemcpyDeviceToHost));
     if (w_half)
-        CUDA_TRY(cudaMemcpy(w_half, s->arena.w_half, sizeof(float) * s->n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(w_half, s->arena.w_half, sizeof(float) * 2 * s->n,
+                            cudaMemcpyDeviceToHost));
     if (raw)
         CUDA_TRY(cudaMemcpy(raw, s->arena.accum, sizeof(int64_t) * kSlots, cudaMemcpyDeviceToHost));
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_set_graphs(vlj_sim* s, int on) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    s->use_graphs = on != 0;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_kernel_timing(vlj_sim* s, int on) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->timing = on != 0;
+    s->ev_used = 0;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_kernel_time(vlj_sim* s, double* total_ms, uint64_t* launches_out) {
+    if (!s || !total_ms || !launches_out) return fail(VLJ_INVALID_ARG, "null argument");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    double total = 0.0;
+    for (size_t k = 0; k < s->ev_used; k++) {
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_start[k], s->ev_end[k]));
+        total += ms;
+    }
+    *total_ms = total;
+    *launches_out = s->ev_used;
+    s->ev_used = 0;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_kernels_executed(vlj_sim* s, uint64_t* n) {
+    if (!s || !n) return fail(VLJ_INVALID_ARG, "null argument");
+    Global g;
+    CUDA_TRY(cudaMemcpyAsync(&g, s->arena.glob, sizeof g, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    *n = g.kernels;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_fp32_peak(double* tflops) {
+    if (!tflops) return fail(VLJ_INVALID_ARG, "null argument");
+    int dev = 0, sms = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t st;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float* out = nullptr;
+    const int blocks = sms * 8, iters = 8192;
+    CUDA_TRY(cudaMalloc(&out, sizeof(float) * blocks));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    double best = 0.0;
+    for (int rep = 0; rep < 6; rep++) {
+        CUDA_TRY(cudaEventRecord(a, st));
+        CUDA_TRY(launch_fp32_peak(out, blocks, iters, st));
+        CUDA_TRY(cudaEventRecord(b, st));
+        CUDA_TRY(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        double flops = 2.0 * 8.0 * (double)iters * (double)blocks * (double)kBlock;
+        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    cudaStreamDestroy(st);
+    *tflops = best;
     return VLJ_OK;
 }
 
@@ -645,14 +731,21 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.sid, seg));
     TRY(dalloc(s, &a.scell, seg));
     TRY(dalloc(s, &a.accum, kSlots));
-    TRY(dalloc(s, &a.pe_half, seg));
-    TRY(dalloc(s, &a.w_half, seg));
+    TRY(dalloc(s, &a.pe_half, 2 * (size_t)seg));
+    TRY(dalloc(s, &a.w_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.vel4, seg));
     TRY(dalloc(s, &a.vcanon, 3 * (size_t)seg));
     // the last cell of the box ends at the last slot
     CUDA_TRY(cudaMemcpy(a.cell_start + a.ncells, &n, sizeof n, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(d_box, &s->box, sizeof(Box), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMallocHost(&s->ring, sizeof(Readback) * kRing));
+    CUDA_TRY(cudaMallocHost(&s->pin_x, sizeof(double) * 3 * (size_t)seg));
+    CUDA_TRY(cudaMallocHost(&s->pin_v, sizeof(double) * 3 * (size_t)seg));
+    CUDA_TRY(cudaMallocHost(&s->pin_id, sizeof(uint32_t) * (size_t)seg));
+    std::memset(s->pin_x, 0, sizeof(double) * 3 * (size_t)seg);
+    std::memset(s->pin_v, 0, sizeof(double) * 3 * (size_t)seg);
+    std::memset(s->pin_id, 0, sizeof(uint32_t) * (size_t)seg);
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking));
     for (int k = 0; k < kRing; k++) {
         CUDA_TRY(cudaEventCreateWithFlags(&s->ring_event[k], cudaEventDisableTiming));
         s->ring_busy[k] = false;
@@ -660,12 +753,88 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     return VLJ_OK;
 }
 
-vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
-    for (uint32_t k = 0; k < steps; k++) {
-        CUDA_TRY(launch_decide(s->arena, s->stream, 0));
-        CUDA_TRY(launch_rebuild(s->arena, s->stream));
+// Ends a capture on `cs`, returning the last captured node in *last.
+static vlj_status end_capture(cudaStream_t cs, cudaError_t launched, cudaGraphNode_t* last) {
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n = 0;
+    cudaError_t info = cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &deps, &n);
+    if (last) *last = (info == cudaSuccess && n == 1) ? deps[0] : nullptr;
+    cudaGraph_t out = nullptr;
+    cudaError_t end = cudaStreamEndCapture(cs, &out);
+    CUDA_TRY(launched);
+    CUDA_TRY(info);
+    CUDA_TRY(end);
+    if (last && !*last) return fail(VLJ_CUDA_ERROR, "graph capture ended with %zu open nodes", n);
+    return VLJ_OK;
+}
+
+// A graph of `count` steps: decide -> IF(some box rebuilds){rebuild chain} ->
+// step kernel, chained. The decide kernel sets the condition on the device,
+// so a step with no rebuild launches no rebuild kernel at all.
+static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaGraphCreate(&g, 0));
+    struct Guard {
+        cudaGraph_t g;
+        ~Guard() { cudaGraphDestroy(g); }
+    } guard{g};
+    cudaStream_t cs = s->capture_stream;
+    const auto mode = cudaStreamCaptureModeThreadLocal;
+    cudaGraphNode_t prev = nullptr;
+    for (uint32_t k = 0; k < count; k++) {
+        cudaGraphConditionalHandle h;
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t n_decide = nullptr, n_cond = nullptr;
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, prev ? &prev : nullptr, nullptr, prev ? 1 : 0,
+                                               mode));
+        TRY(end_capture(cs, launch_decide(s->arena, cs, h), &n_decide));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        CUDA_TRY(cudaGraphAddNode(&n_cond, g, &n_decide, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
+        TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
+        TRY(end_capture(cs, launch_step(s->arena, s->shifted_force, cs), &prev));
+    }
+    CUDA_TRY(cudaGraphInstantiate(out, g, 0));
+    return VLJ_OK;
+}
+
+static vlj_status step_direct(vlj_sim* s) {
+    CUDA_TRY(launch_decide(s->arena, s->stream, 0));
+    CUDA_TRY(launch_rebuild(s->arena, s->stream));
+    if (s->timing) {
+        if (s->ev_used == s->ev_start.size()) {
+            cudaEvent_t a, b;
+            CUDA_TRY(cudaEventCreate(&a));
+            CUDA_TRY(cudaEventCreate(&b));
+            s->ev_start.push_back(a);
+            s->ev_end.push_back(b);
+        }
+        CUDA_TRY(cudaEventRecord(s->ev_start[s->ev_used], s->stream));
+        CUDA_TRY(launch_step(s->arena, s->shifted_force, s->stream));
+        CUDA_TRY(cudaEventRecord(s->ev_end[s->ev_used], s->stream));
+        s->ev_used++;
+    } else {
         CUDA_TRY(launch_step(s->arena, s->shifted_force, s->stream));
     }
+    return VLJ_OK;
+}
+
+vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
+    if (s->timing || !s->use_graphs) {
+        for (uint32_t k = 0; k < steps; k++) TRY(step_direct(s));
+        return VLJ_OK;
+    }
+    if (!s->graph_chunk) TRY(build_graph(s, kGraphChunk, &s->graph_chunk));
+    if (!s->graph_one) TRY(build_graph(s, 1, &s->graph_one));
+    for (; steps >= kGraphChunk; steps -= kGraphChunk)
+        CUDA_TRY(cudaGraphLaunch(s->graph_chunk, s->stream));
+    for (; steps > 0; steps--) CUDA_TRY(cudaGraphLaunch(s->graph_one, s->stream));
     return VLJ_OK;
 }
 

@@ -49,6 +49,8 @@ struct Box {
     float shift, force_shift, rc;
     float energy_scale, momentum_scale;
     float bin_width;
+    float inv_box_f[3];  // 1 / box_f, for nearest_ref_fast
+    float prefilter_r2;  // list_r2 widened past any encoding difference
     uint32_t cells[3];
     uint32_t total_cells;
     uint32_t cell_base;  // first cell of this box
@@ -82,7 +84,8 @@ struct Global {
     uint32_t pending;    // a step finished since the last decision
     uint32_t any;        // some box rebuilds this step
     uint32_t fault;      // first error a kernel recorded (0 none)
-    unsigned long long step;  // steps taken: the counter of the noise stream
+    unsigned long long step;     // steps taken: the counter of the noise stream
+    unsigned long long kernels;  // kernels of this arena that ran
 };
 
 // Every pointer a kernel needs; passed by value (it sits in the constant
@@ -118,8 +121,8 @@ struct Arena {
     uint32_t* scell;
     // measurements
     unsigned long long* accum;  // nboxes * kSlots
-    float* pe_half;
-    float* w_half;
+    float* pe_half;  // (hi, lo) per slot
+    float* w_half;   // (hi, lo) per slot
     float4* vel4;
     double* vcanon;             // canonical velocities (3 * seg), on request
     // profiles / heat current
@@ -215,28 +218,55 @@ __device__ __forceinline__ float3 langevin_noise(uint32_t id, unsigned long long
     return make_float3(ra * cosf(aa), ra * sinf(aa), rb * cosf(ab));
 }
 
-// r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545)
+// r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545). The
+// reciprocal and square root are the hardware approximations (about 1 ulp),
+// well inside the f32 pair arithmetic's own error.
 template <bool SHIFTED_FORCE>
 __device__ __forceinline__ void lj_pair(float r2, const Box& b, float& rf, float& u) {
-    float inv2 = 1.0f / r2;
+    float inv2 = __fdividef(1.0f, r2);
     float s6 = inv2 * inv2 * inv2;
     float s12 = s6 * s6;
     rf = 24.0f * (2.0f * s12 - s6);
     u = 4.0f * (s12 - s6) - b.shift;
     if (SHIFTED_FORCE) {
-        float r = sqrtf(r2);
+        float r = r2 * rsqrtf(r2);
         rf -= r * b.force_shift;
         u += (r - b.rc) * b.force_shift;
     }
 }
 
+// |F| / r of a pair at r2 < rc2: the factor that multiplies the separation.
 template <bool SHIFTED_FORCE>
-__device__ __forceinline__ float lj_force_over_r2(float r2, const Box& b) {
-    float inv2 = 1.0f / r2;
+__device__ __forceinline__ float lj_force_over_r2(float r2, float force_shift) {
+    float inv2 = __fdividef(1.0f, r2);
     float s6 = inv2 * inv2 * inv2;
     float rf = 24.0f * s6 * (2.0f * s6 - 1.0f);
-    if (SHIFTED_FORCE) rf -= sqrtf(r2) * b.force_shift;
+    if (SHIFTED_FORCE) rf -= r2 * rsqrtf(r2) * force_shift;
     return rf * inv2;
+}
+
+// The reference's nearest image d - side * round(d / side) with the IEEE
+// quotient, computed through the reciprocal: d * (1 / side) is within 2e-7 of
+// d / side for |d| <= side, so both round to the same integer unless the
+// quotient is within 1e-6 of a half-integer, where the exact division is
+// taken. Bit-identical to nearest_ref.
+__device__ __forceinline__ float nearest_ref_fast(float d, float side, float inv_side) {
+    float q = d * inv_side;
+    float aq = fabsf(q);
+    float r;
+    if (aq < 1.25f && fabsf(aq - 0.5f) > 1e-6f)
+        r = rintf(q);
+    else
+        r = rintf(__fdiv_rn(d, side));
+    return __fsub_rn(d, __fmul_rn(side, r));
+}
+
+// Squared length of an encoded separation (the force kernels' arithmetic).
+__device__ __forceinline__ float encoded_r2(uint4 a, uint4 b, const float dec[3]) {
+    float dx = decode_diff(a.x, b.x, dec[0]);
+    float dy = decode_diff(a.y, b.y, dec[1]);
+    float dz = decode_diff(a.z, b.z, dec[2]);
+    return dx * dx + dy * dy + dz * dz;
 }
 
 // ---- launchers (vlj_kernels.cu); every kernel takes the Arena by value ----
@@ -248,6 +278,7 @@ cudaError_t launch_step(const Arena& a, bool shifted_force, cudaStream_t s);
 cudaError_t launch_measure(const Arena& a, bool shifted_force, bool canonical, cudaStream_t s);
 cudaError_t launch_profile(const Arena& a, bool shifted_force, cudaStream_t s);
 cudaError_t launch_heat_current(const Arena& a, bool shifted_force, cudaStream_t s);
+cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s);
 unsigned long long launches();
 
 }  // namespace vlj

@@ -38,6 +38,12 @@ __device__ __forceinline__ uint32_t box_of_cell(const Arena& a, uint32_t cell) {
     return a.box_of_cell ? a.box_of_cell[cell] : 0u;
 }
 
+// Every kernel counts its own launch once, so the number of this library's
+// kernels that ran (graph nodes skipped by a condition do not) is exact.
+__device__ __forceinline__ void count_kernel(const Arena& a) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.glob->kernels, 1ull);
+}
+
 __device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
     return a.ctrl[b].rebuild != 0u;
 }
@@ -114,6 +120,7 @@ __device__ __forceinline__ void block_sum_slots(const Arena& a, bool valid, uint
 
 // ---- encode positions into the current cache copy ----
 __global__ void encode_kernel(Arena a) {
+    count_kernel(a);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
     const Box& bx = a.boxes[box_of_slot(a, i)];
@@ -132,6 +139,7 @@ __global__ void encode_kernel(Arena a) {
 // reorder_every-th rebuild (counted before the increment, as the reference).
 template <bool SET_CONDITION>
 __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
+    count_kernel(a);
     __shared__ int s_any;
     Global* g = a.glob;
     if (threadIdx.x == 0) {
@@ -169,6 +177,7 @@ __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
 
 // ---- bin (grid.wgsl:11-38): cell of each slot from its f32 position ----
 __global__ void bin_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
@@ -195,6 +204,7 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t b = blockIdx.x;
     if (b >= a.nboxes || !rebuilding(a, b)) return;
@@ -251,6 +261,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
 
 // ---- scatter (grid.wgsl:119-127): slot into its cell's next free place ----
 __global__ void scatter_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
@@ -278,6 +289,7 @@ __device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, u
 }
 
 __global__ void sort_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -331,6 +343,7 @@ __global__ void sort_kernel(Arena a) {
 
 // ---- reorder copy back (lennard_jones.wgsl:435-452) ----
 __global__ void reorder_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nslots) return;
@@ -358,6 +371,7 @@ __global__ void reorder_kernel(Arena a) {
 // ---- the reference's packed positions for the list build
 // (lennard_jones.wgsl:154-164; hi/lo as Df64::from_f64, lennard_jones.rs:476-489)
 __global__ void pack_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nslots) return;
@@ -377,24 +391,37 @@ __global__ void pack_kernel(Arena a) {
 
 // ---- Verlet list build (lennard_jones.wgsl:454-499) ----
 // Everything within cutoff + skin, cells in the order dz, dy, dx = -1..1 with
-// periodic wrap, then each cell in sorted order; the distance test is the
-// reference's f32 arithmetic on packed positions, operation for operation.
-__global__ void build_list_kernel(Arena a) {
+// periodic wrap, then each cell in sorted order. The membership test is the
+// reference's f32 arithmetic on packed positions, operation for operation, so
+// the lists are the reference's bit for bit. It runs only on candidates that
+// pass a cheaper test on the 32-bit encoded positions against a radius
+// widened past any difference between the two encodings (prefilter_r2).
+__global__ void __launch_bounds__(kBlock) build_list_kernel(Arena a) {
+    count_kernel(a);
     if (!a.glob->any) return;
+    __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
+    for (int t = threadIdx.x; t < 512; t += blockDim.x)
+        s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
+    __syncthreads();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
     uint32_t b = box_of_slot(a, i);
     if (!rebuilding(a, b)) return;
     const Box& bx = a.boxes[b];
+    const uint4* __restrict__ cur = a.cache[a.glob->phase];
+    const uint4 own_enc = cur[i];
     const float4 own = a.ref[i];
     const float4 own_lo = a.ref_lo[i];
     const float xh[3] = {own.x, own.y, own.z};
     const float xl[3] = {own_lo.x, own_lo.y, own_lo.z};
+    const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
+    const float side[3] = {bx.box_f[0], bx.box_f[1], bx.box_f[2]};
+    const float inv[3] = {bx.inv_box_f[0], bx.inv_box_f[1], bx.inv_box_f[2]};
     const int32_t nx = (int32_t)bx.cells[0], ny = (int32_t)bx.cells[1], nz = (int32_t)bx.cells[2];
     const int32_t ci = (int32_t)(a.cell_of_slot[i] - bx.cell_base);
     const int32_t cx = ci % nx, cy = (ci / nx) % ny, cz = ci / (nx * ny);
     const uint32_t cap = bx.capacity;
-    const float list_r2 = bx.list_r2;
+    const float list_r2 = bx.list_r2, pre_r2 = bx.prefilter_r2;
     uint32_t found = 0;
     for (int32_t dz = -1; dz <= 1; dz++)
         for (int32_t dy = -1; dy <= 1; dy++)
@@ -407,19 +434,19 @@ __global__ void build_list_kernel(Arena a) {
                 for (uint32_t t = a.cell_start[cell]; t < end; t++) {
                     uint32_t j = a.sorted[t];
                     if (j == i) continue;
+                    if (encoded_r2(__ldg(cur + j), own_enc, dec) >= pre_r2) continue;
                     float4 pj = a.ref[j];
                     uint32_t bits = __float_as_uint(pj.w);
-                    float d0 = nearest_ref(__fadd_rn(__fsub_rn(pj.x, xh[0]),
-                                                     __fsub_rn(unpack_lo1(pj.x, bits, 0), xl[0])),
-                                           bx.box_f[0]);
-                    float d1 = nearest_ref(__fadd_rn(__fsub_rn(pj.y, xh[1]),
-                                                     __fsub_rn(unpack_lo1(pj.y, bits, 1), xl[1])),
-                                           bx.box_f[1]);
-                    float d2 = nearest_ref(__fadd_rn(__fsub_rn(pj.z, xh[2]),
-                                                     __fsub_rn(unpack_lo1(pj.z, bits, 2), xl[2])),
-                                           bx.box_f[2]);
-                    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)),
-                                         __fmul_rn(d2, d2));
+                    const float ph[3] = {pj.x, pj.y, pj.z};
+                    float d[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        float lo = __fmul_rn(s_q510[(bits >> (9u * k)) & 511u], last_bit(ph[k]));
+                        float e = __fadd_rn(__fsub_rn(ph[k], xh[k]), __fsub_rn(lo, xl[k]));
+                        d[k] = nearest_ref_fast(e, side[k], inv[k]);
+                    }
+                    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])),
+                                         __fmul_rn(d[2], d[2]));
                     if (r2 < list_r2) {
                         if (found < cap) a.list[(size_t)found * a.seg + i] = j;
                         found += 1;
@@ -428,23 +455,36 @@ __global__ void build_list_kernel(Arena a) {
             }
     a.list_count[i] = found < cap ? found : cap;
     if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
-    a.snap[i] = a.cache[a.glob->phase][i];
+    a.snap[i] = own_enc;
 }
 
 // ---- forces from the list (lennard_jones.wgsl:503-530) ----
 // Separations come from the 32-bit box fractions: the wrapped integer
 // difference is the nearest image.
+// Error-free sum s + e = a + b (Knuth's two-sum; df64.rs:15-22).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// With ENERGIES, each particle's halves of its pair energies and virials are
+// summed as unevaluated f32 pairs (pe + pe_lo, w + w_lo), as the reference
+// sums them in double-float (lennard_jones.wgsl:518-519); both parts go to
+// fixed point separately.
 template <bool SHIFTED_FORCE, bool ENERGIES>
 __device__ __forceinline__ void pair_sums(const Arena& a, const Box& bx, uint32_t i,
                                           const uint4* __restrict__ cur, float& ax, float& ay,
-                                          float& az, float& pe, float& w, uint32_t& near) {
+                                          float& az, float& pe, float& pe_lo, float& w,
+                                          float& w_lo, uint32_t& near) {
     const uint4 own = __ldg(cur + i);
     const uint32_t cnt = __ldg(a.list_count + i);
     const uint32_t* __restrict__ row = a.list + i;
     const size_t seg = a.seg;
     const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
+    const float fshift = bx.force_shift;
     ax = ay = az = 0.0f;
-    pe = w = 0.0f;
+    pe = w = pe_lo = w_lo = 0.0f;
     near = 0;
     for (uint32_t k = 0; k < cnt; k++) {
         const uint32_t j = __ldg(row + k * seg);
@@ -458,12 +498,17 @@ __device__ __forceinline__ void pair_sums(const Arena& a, const Box& bx, uint32_
             if (ENERGIES) {
                 float rf, u;
                 lj_pair<SHIFTED_FORCE>(r2, bx, rf, u);
-                f = rf / r2;
-                pe += 0.5f * u;
-                w += 0.5f * rf;
+                f = __fdividef(rf, r2);
+                float t, e;
+                two_sum(pe, 0.5f * u, t, e);
+                pe = t;
+                pe_lo += e;
+                two_sum(w, 0.5f * rf, t, e);
+                w = t;
+                w_lo += e;
                 near += r2 < 2.25f ? 1u : 0u;
             } else {
-                f = lj_force_over_r2<SHIFTED_FORCE>(r2, bx);
+                f = lj_force_over_r2<SHIFTED_FORCE>(r2, fshift);
             }
             ax -= dx * f;
             ay -= dy * f;
@@ -483,13 +528,14 @@ __device__ __forceinline__ double wrap(double x, double side) {
 // becomes half a kick behind the given one ----
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kBlock) prime_kernel(Arena a) {
+    count_kernel(a);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
     const Box& bx = a.boxes[box_of_slot(a, i)];
     const uint4* cur = a.cache[a.glob->phase];
-    float ax, ay, az, pe, w;
+    float ax, ay, az, pe, pe_lo, w, w_lo;
     uint32_t near;
-    pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, w, near);
+    pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, pe_lo, w, w_lo, near);
     a.v[i] -= (double)ax * bx.half_dt;
     a.v[a.seg + i] -= (double)ay * bx.half_dt;
     a.v[2 * a.seg + i] -= (double)az * bx.half_dt;
@@ -504,6 +550,7 @@ __global__ void __launch_bounds__(kBlock) prime_kernel(Arena a) {
 // Philox stream keyed by (seed, step, particle id). All state updates in f64.
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kBlock) step_kernel(Arena a) {
+    count_kernel(a);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < a.nslots;
     const uint32_t phase = a.glob->phase;
@@ -514,9 +561,9 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Arena a) {
     if (valid) {
         b = box_of_slot(a, i);
         const Box& bx = a.boxes[b];
-        float ax, ay, az, pe, w;
+        float ax, ay, az, pe, pe_lo, w, w_lo;
         uint32_t near;
-        pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, w, near);
+        pair_sums<SHIFTED_FORCE, false>(a, bx, i, cur, ax, ay, az, pe, pe_lo, w, w_lo, near);
         const float acc[3] = {ax, ay, az};
         float3 xi = make_float3(0.0f, 0.0f, 0.0f);
         const bool langevin = bx.thermostat == 1;
@@ -556,6 +603,7 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Arena a) {
 // to 32.32 fixed point scaled like the reference and is summed exactly.
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, int canonical) {
+    count_kernel(a);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < a.nslots;
     uint32_t b = 0;
@@ -564,9 +612,9 @@ __global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, int canonical)
         b = box_of_slot(a, i);
         const Box& bx = a.boxes[b];
         const uint4* cur = a.cache[a.glob->phase];
-        float ax, ay, az, pe, w;
+        float ax, ay, az, pe, pe_lo, w, w_lo;
         uint32_t near;
-        pair_sums<SHIFTED_FORCE, true>(a, bx, i, cur, ax, ay, az, pe, w, near);
+        pair_sums<SHIFTED_FORCE, true>(a, bx, i, cur, ax, ay, az, pe, pe_lo, w, w_lo, near);
         const float acc[3] = {ax, ay, az};
         double vel[3], ke = 0.0;
 #pragma unroll
@@ -577,13 +625,15 @@ __global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, int canonical)
         ke *= 0.5;
         const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
         v[0] = fixed_raw_f64(ke * es);
-        v[1] = fixed_raw_f32(pe * bx.energy_scale);
-        v[2] = fixed_raw_f32(w * bx.energy_scale);
+        v[1] = fixed_raw_f32(pe * bx.energy_scale) + fixed_raw_f32(pe_lo * bx.energy_scale);
+        v[2] = fixed_raw_f32(w * bx.energy_scale) + fixed_raw_f32(w_lo * bx.energy_scale);
 #pragma unroll
         for (int k = 0; k < 3; k++) v[3 + k] = fixed_raw_f64(vel[k] * ms);
         v[6] = near >= bx.near_count ? (1ll << 32) : 0ll;
-        a.pe_half[i] = pe;
-        a.w_half[i] = w;
+        a.pe_half[2 * i] = pe;
+        a.pe_half[2 * i + 1] = pe_lo;
+        a.w_half[2 * i] = w;
+        a.w_half[2 * i + 1] = w_lo;
         a.vel4[i] = make_float4((float)vel[0], (float)vel[1], (float)vel[2], (float)near);
         if (canonical) {
 #pragma unroll
@@ -591,6 +641,28 @@ __global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, int canonical)
         }
     }
     block_sum_slots(a, valid, b, v);
+}
+
+// ---- FP32 calibration: eight independent FMA chains per thread, so the
+// FMA pipes stay full; 2 flops per FMA ----
+__global__ void __launch_bounds__(kBlock) fp32_peak_kernel(float* out, int iters) {
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = (float)(threadIdx.x + k) * 1e-3f;
+    const float m = 0.999999f, c = 1e-6f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = fmaf(a[k], m, c);
+    }
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) t += a[k];
+    if (t == 12345.678f) out[blockIdx.x] = t;  // keeps the chains live
+}
+
+cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s) {
+    fp32_peak_kernel<<<blocks, kBlock, 0, s>>>(out, iters);
+    return after_launch();
 }
 
 // ---- launchers ----

@@ -11,6 +11,7 @@
 namespace vlj {
 
 constexpr int kRing = 3;  // measurement read-back slots (lennard_jones.rs:320)
+constexpr uint32_t kGraphChunk = 16;  // steps per graph launch
 
 // One measurement's words as read back into pinned host memory.
 struct Readback {
@@ -46,10 +47,20 @@ struct vlj_sim {
     uint64_t profile_samples = 0;
     // heat current series
     uint32_t series_samples = 0;
-    // captured steps
-    cudaGraph_t step_graph = nullptr;
-    cudaGraphExec_t step_graph_exec = nullptr;
-    uint32_t graph_steps = 0;
+    // pinned staging for particle uploads and read-backs (x, v: 3 * seg; id: seg)
+    double* pin_x = nullptr;
+    double* pin_v = nullptr;
+    uint32_t* pin_id = nullptr;
+    // captured steps: a graph of kGraphChunk steps and one of a single step,
+    // each step's rebuild chain under a conditional node
+    bool use_graphs = true;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graph_chunk = nullptr;
+    cudaGraphExec_t graph_one = nullptr;
+    // per-launch timing of the step kernel (direct launches while on)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_start, ev_end;
+    size_t ev_used = 0;
 
     ~vlj_sim();
 };

@@ -55,6 +55,13 @@ def device_count():
     return n.value
 
 
+def fp32_peak():
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    t = C.c_double()
+    _check(_lib.vlj_debug_fp32_peak(C.byref(t)))
+    return t.value
+
+
 def launches():
     """Kernel launches this library has made in this process."""
     n = C.c_uint64()
@@ -424,12 +431,30 @@ class LennardJones:
                        ("sorted", "cell_start", "cell_of_slot", "ids", "counts", "lists", "x", "v")]))
         return out
 
+    def set_graphs(self, on):
+        _check(_lib.vlj_debug_set_graphs(self._h, int(bool(on))))
+
+    def kernel_timing(self, on):
+        _check(_lib.vlj_debug_kernel_timing(self._h, int(bool(on))))
+
+    def kernel_time(self):
+        """(total ms, launches) of the step kernel since timing was switched on."""
+        ms, n = C.c_double(), C.c_uint64()
+        _check(_lib.vlj_debug_kernel_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def kernels_executed(self):
+        n = C.c_uint64()
+        _check(_lib.vlj_debug_kernels_executed(self._h, C.byref(n)))
+        return n.value
+
     def force_rebuild(self):
         _check(_lib.vlj_debug_force_rebuild(self._h))
 
     def read_partials(self):
-        pe = np.zeros(self._n, np.float32)
-        w = np.zeros(self._n, np.float32)
+        """(pe, w, raw): per-slot (hi, lo) halves of pair energy and virial."""
+        pe = np.zeros((self._n, 2), np.float32)
+        w = np.zeros((self._n, 2), np.float32)
         raw = np.zeros(8, np.int64)
         _check(_lib.vlj_debug_read_partials(self._h, _ffi.ptr(pe), _ffi.ptr(w), _ffi.ptr(raw)))
         return pe, w, raw
