@@ -109,10 +109,13 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
     b.list_r2 = (float)(list_radius * list_radius);
     b.half_skin2 = (float)(0.25 * skin * skin);
     // The reference's f32 separations can be off by a few units in the last
-    // place of the box side for pairs across the boundary; widen past that.
+    // place of the box side (pairs across the boundary); the encoded ones by
+    // far less. Bracket the list radius by more than both.
     double side_max = std::max(b.box[0], std::max(b.box[1], b.box[2]));
-    double pre_r = std::sqrt((double)b.list_r2) + 8.0 * std::ldexp(1.0, std::ilogb(side_max) - 23) + 1e-4;
-    b.prefilter_r2 = (float)(pre_r * pre_r);
+    double margin = 8.0 * std::ldexp(1.0, std::ilogb(side_max) - 23) + 1e-4;
+    double list_r = std::sqrt((double)b.list_r2);
+    b.prefilter_r2 = (float)((list_r + margin) * (list_r + margin));
+    b.accept_r2 = (float)((list_r - margin) * (list_r - margin));
     for (int k = 0; k < 3; k++) b.inv_box_f[k] = 1.0f / b.box_f[k];
     b.dt = dt;
     b.half_dt = 0.5 * dt;
@@ -208,7 +211,7 @@ vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_encode(s->arena, s->stream));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
-    CUDA_TRY(launch_prime(s->arena, s->shifted_force, s->stream));
+    CUDA_TRY(launch_prime(s->arena, s->list_map, s->shifted_force, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return VLJ_OK;
 }
@@ -243,7 +246,7 @@ vlj_measurement decode(const vlj_sim* s, const Readback& r, uint64_t step) {
 vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
     CUDA_TRY(cudaMemsetAsync(s->arena.accum, 0, sizeof(unsigned long long) * kSlots, s->stream));
     TRY(lists_now(s));
-    CUDA_TRY(launch_measure(s->arena, s->shifted_force, canonical, s->stream));
+    CUDA_TRY(launch_measure(s->arena, s->list_map, s->shifted_force, canonical, s->stream));
     if (slot >= 0) {
         Readback* r = &s->ring[slot];
         CUDA_TRY(cudaMemcpyAsync(r->slots, s->arena.accum, sizeof(r->slots), cudaMemcpyDeviceToHost,
@@ -346,7 +349,7 @@ vlj_status vlj_run(vlj_sim* s, uint64_t steps) {
         steps -= batch;
     }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    return VLJ_OK;
+    return check_fault(s);
 }
 
 vlj_status vlj_measure(vlj_sim* s, int* accepted) {
@@ -398,7 +401,7 @@ vlj_status vlj_measure_now(vlj_sim* s, vlj_measurement* out) {
     TRY(vlj_poll(s, buf, kRing, &n));
     if (n == 0) return fail(VLJ_CUDA_ERROR, "the measurement did not finish");
     *out = buf[n - 1];
-    return VLJ_OK;
+    return check_fault(s);
 }
 
 vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
@@ -563,10 +566,11 @@ vlj_status vlj_debug_read_grid(vlj_sim* s, uint32_t* sorted, uint32_t* cell_star
     TRY(get(ids, s->arena.id, sizeof(uint32_t) * n));
     TRY(get(list_count, s->arena.list_count, sizeof(uint32_t) * n));
     if (list) {
-        std::vector<uint32_t> t(seg * cap);
-        TRY(get(t.data(), s->arena.list, sizeof(uint32_t) * seg * cap));
+        const size_t rows = (cap + 3) / 4;
+        std::vector<uint32_t> t(seg * rows * 4);
+        TRY(get(t.data(), s->arena.list, sizeof(uint32_t) * t.size()));
         for (size_t i = 0; i < n; i++)
-            for (size_t k = 0; k < cap; k++) list[i * cap + k] = t[k * seg + i];
+            for (size_t k = 0; k < cap; k++) list[i * cap + k] = t[((k / 4) * seg + i) * 4 + k % 4];
     }
     if (pos || vel_stored) {
         std::vector<double> x(3 * seg), v(3 * seg);
@@ -686,6 +690,42 @@ vlj_status vlj_debug_launches(uint64_t* n) {
 // ---- allocation and step enqueue (shared with the graph path) ----
 namespace vlj {
 
+// The 2D tensor map the force kernels stage list rows through: inner
+// dimension 4 * seg u32 (four entries of every slot), outer one row per four
+// list entries; box kStageRows rows of kBlockParticles slots. Row stride
+// 16 * seg bytes (seg is a multiple of 16, so 16-byte aligned as TMA needs).
+vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return fail(VLJ_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)a.seg * 4u, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)a.seg * 16u};
+    const cuuint32_t box[2] = {(cuuint32_t)kBlockParticles * 4u, (cuuint32_t)kStageRows};
+    const cuuint32_t estrides[2] = {1u, 1u};
+    CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, a.list, dims, strides, box, estrides,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VLJ_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return VLJ_OK;
+}
+
+// VLJ_TIMEOUT when a kernel recorded a fault (a TMA tile that never arrived).
+vlj_status check_fault(vlj_sim* s) {
+    Global g;
+    CUDA_TRY(cudaMemcpyAsync(&g, s->arena.glob, sizeof g, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (g.fault == kFaultTmaTimeout)
+        return fail(VLJ_TIMEOUT, "a list tile did not arrive within the wait limit");
+    if (g.fault) return fail(VLJ_CUDA_ERROR, "kernel fault code %u", g.fault);
+    return VLJ_OK;
+}
+
 vlj_status sim_allocate(vlj_sim* s, void* stream) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
@@ -725,7 +765,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));
     TRY(dalloc(s, &a.count, a.ncells));
     TRY(dalloc(s, &a.list_count, seg));
-    TRY(dalloc(s, &a.list, (size_t)seg * s->box.capacity));
+    TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((s->box.capacity + 3) / 4)));
+    TRY(make_list_map(a, (s->box.capacity + 3) / 4, &s->list_map));
     TRY(dalloc(s, &a.sx, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sv, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sid, seg));
@@ -798,7 +839,7 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
         TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
-        TRY(end_capture(cs, launch_step(s->arena, s->shifted_force, cs), &prev));
+        TRY(end_capture(cs, launch_step(s->arena, s->list_map, s->shifted_force, cs), &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
     return VLJ_OK;
@@ -816,11 +857,11 @@ static vlj_status step_direct(vlj_sim* s) {
             s->ev_end.push_back(b);
         }
         CUDA_TRY(cudaEventRecord(s->ev_start[s->ev_used], s->stream));
-        CUDA_TRY(launch_step(s->arena, s->shifted_force, s->stream));
+        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream));
         CUDA_TRY(cudaEventRecord(s->ev_end[s->ev_used], s->stream));
         s->ev_used++;
     } else {
-        CUDA_TRY(launch_step(s->arena, s->shifted_force, s->stream));
+        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream));
     }
     return VLJ_OK;
 }

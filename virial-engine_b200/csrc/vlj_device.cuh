@@ -1,0 +1,118 @@
+// Device helpers shared by the kernel sources (vlj_grid.cu, vlj_forces.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+// Host side: grid size for n threads, and launch bookkeeping (vlj_grid.cu).
+inline unsigned blocks_for(uint64_t n, int threads = kBlock) {
+    uint64_t b = (n + (uint64_t)threads - 1) / (uint64_t)threads;
+    return b ? (unsigned)b : 1u;
+}
+cudaError_t after_launch(unsigned n = 1);
+
+__device__ __forceinline__ uint32_t box_of_slot(const Arena& a, uint32_t slot) {
+    return a.box_of_slot ? a.box_of_slot[slot] : 0u;
+}
+
+__device__ __forceinline__ uint32_t box_of_cell(const Arena& a, uint32_t cell) {
+    return a.box_of_cell ? a.box_of_cell[cell] : 0u;
+}
+
+// Every kernel counts its own launch once, so the number of this library's
+// kernels that ran (graph nodes skipped by a condition do not) is exact.
+__device__ __forceinline__ void count_kernel(const Arena& a) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.glob->kernels, 1ull);
+}
+
+__device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
+    return a.ctrl[b].rebuild != 0u;
+}
+
+// Whether every valid thread of the block belongs to the box of the block's
+// first slot; that box in *ref. Call from every thread of the block.
+__device__ __forceinline__ bool block_in_one_box(const Arena& a, bool valid, uint32_t b,
+                                                 uint32_t first_slot, uint32_t* ref) {
+    __shared__ uint32_t s_ref;
+    __shared__ int s_mixed;
+    if (threadIdx.x == 0) {
+        s_mixed = 0;
+        s_ref = box_of_slot(a, first_slot);
+    }
+    __syncthreads();
+    if (valid && b != s_ref) s_mixed = 1;
+    __syncthreads();
+    *ref = s_ref;
+    return s_mixed == 0;
+}
+
+// Largest value over the block into each box's max_disp: one atomicMax when
+// the block lies in one box (the usual case), one per thread otherwise.
+__device__ __forceinline__ void block_max_per_box(const Arena& a, bool valid, uint32_t b,
+                                                  uint32_t first_slot, float value) {
+    __shared__ uint32_t s_val[kBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t bits = valid ? __float_as_uint(value) : 0u;
+    uint32_t ref;
+    if (!block_in_one_box(a, valid, b, first_slot, &ref)) {
+        if (valid) atomicMax(&a.ctrl[b].max_disp, bits);
+        return;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bits = max(bits, __shfl_xor_sync(0xffffffffu, bits, o));
+    if (lane == 0) s_val[warp] = bits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = max(m, s_val[w]);
+        atomicMax(&a.ctrl[ref].max_disp, m);
+    }
+}
+
+// Sum of kSlots 64-bit integers over the block into each box's accumulators,
+// with the same one-box shortcut. Integer sums: the order does not matter.
+__device__ __forceinline__ void block_sum_slots(const Arena& a, bool valid, uint32_t b,
+                                                uint32_t first_slot, long long (&v)[kSlots]) {
+    __shared__ long long s_sum[kBlock / 32][kSlots];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t ref;
+    if (!block_in_one_box(a, valid, b, first_slot, &ref)) {
+        if (valid)
+            for (int k = 0; k < kSlots; k++)
+                if (v[k]) atomicAdd(&a.accum[b * kSlots + k], (unsigned long long)v[k]);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kSlots; k++) {
+        long long x = valid ? v[k] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) s_sum[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kSlots) {
+        long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_sum[w][threadIdx.x];
+        if (t) atomicAdd(&a.accum[ref * kSlots + threadIdx.x], (unsigned long long)t);
+    }
+}
+
+// Error-free sum s + e = a + b (Knuth's two-sum; df64.rs:15-22).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// Periodic wrap of an f64 coordinate that moved less than one side.
+__device__ __forceinline__ double wrap(double x, double side) {
+    if (x >= side) x -= side;
+    if (x < 0.0) x += side;
+    if (x >= side) x -= side;
+    return x;
+}
+
+}  // namespace vlj

@@ -1,0 +1,406 @@
+// CUDA kernels of the pair forces, the integrator and the measurements,
+// sm_100a.
+//
+// Four lanes of a warp serve one particle. A block serves 64 consecutive
+// slots; their Verlet-list rows (16 B per slot per row, four entries) stream
+// from HBM into shared memory as TMA tiles of 8 rows x 64 slots, three tiles
+// in flight per block, so the list -- most of the step's HBM traffic -- moves
+// asynchronously while the lanes work. Each lane takes one entry of every row
+// (every fourth list entry), gathers the neighbour's encoded position through
+// L1, and the four lanes' sums are combined by warp shuffles in a fixed
+// pattern, so every rerun adds in the same order. Lanes 0, 1 and 2 then
+// update the x, y and z coordinate. Reference kernels are cited at each kernel.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "vlj_device.cuh"
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kTileBytes = kStageRows * kBlockParticles * 16u;
+constexpr unsigned long long kWaitLimitNs = 500000000ull;  // 0.5 s per TMA tile
+
+struct PairSums {
+    float ax, ay, az;
+    float pe, pe_lo;  // this particle's half of its pair energies, hi + lo
+    float w, w_lo;    // and of its pair virials r . F
+    uint32_t near;    // neighbours within 1.5 sigma
+};
+
+// Shared memory of a force-kernel block: the tile ring and its barriers.
+struct Stage {
+    uint4 rows[kStageSlots][kStageRows][kBlockParticles];
+    unsigned long long bar[kStageSlots];
+};
+
+// ---- TMA and mbarrier primitives (PTX, sm_90+) ----
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One tile: rows [y, y + kStageRows) of slots [x / 4, x / 4 + 64). Rows and
+// slots past the list's end arrive as zeros. No multicast.
+__device__ __forceinline__ void tile_load(const CUtensorMap* map, void* dst, unsigned long long* bar,
+                                          int x, int y) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_addr(bar)), "r"(kTileBytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for a tile with a time limit; false when it did not arrive.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
+    if (bar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!bar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    return true;
+}
+
+// ---- forces from the list (lennard_jones.wgsl:503-545) ----
+// Separations come from the 32-bit box fractions: the wrapped integer
+// difference is the nearest image. The force factor is the same expression
+// in every pass, so the step, the first forces and the measurement agree to
+// the bit. With ENERGIES each lane also sums its halves of pair energy and
+// virial as unevaluated f32 pairs (as the reference sums them in
+// double-float, lennard_jones.wgsl:518-519). Every thread of the block must
+// call this (it synchronises the block and ends in shuffles); on return the
+// four lanes of a particle hold its totals.
+template <bool SHIFTED_FORCE, bool ENERGIES>
+__device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap* map,
+                                                    const Arena& a, const Box& bx, uint32_t i,
+                                                    uint32_t sub, bool valid,
+                                                    const uint4* __restrict__ cur) {
+    PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u};
+    const uint32_t first = blockIdx.x * kBlockParticles;
+    const uint32_t p = threadIdx.x / kLanes;
+    const uint32_t rows = (a.glob->max_count + 3u) / 4u;
+    const uint32_t tiles = (rows + kStageRows - 1u) / kStageRows;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kStageSlots; k++) bar_init(&st.bar[k]);
+        init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (uint32_t t = 0; t < tiles && t < (uint32_t)kStageSlots; t++)
+            tile_load(map, &st.rows[t][0][0], &st.bar[t], (int)(first * 4u), (int)(t * kStageRows));
+
+    uint4 own = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t cnt = 0;
+    if (valid) {
+        own = __ldg(cur + i);
+        cnt = __ldg(a.list_count + i);
+    }
+    const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
+    const float fshift = bx.force_shift;
+    auto accumulate = [&](const uint4 pj) {
+        const float dx = decode_diff(pj.x, own.x, dec0);
+        const float dy = decode_diff(pj.y, own.y, dec1);
+        const float dz = decode_diff(pj.z, own.z, dec2);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const bool in = r2 < rc2;
+        // branch-free: most list entries are inside the cutoff and the pair
+        // math is finite for all of them
+        const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
+        s.ax -= dx * f;
+        s.ay -= dy * f;
+        s.az -= dz * f;
+        if (ENERGIES && in) {
+            float rf, u, t, e;
+            lj_pair<SHIFTED_FORCE>(r2, bx, rf, u);
+            two_sum(s.pe, 0.5f * u, t, e);
+            s.pe = t;
+            s.pe_lo += e;
+            two_sum(s.w, 0.5f * rf, t, e);
+            s.w = t;
+            s.w_lo += e;
+            s.near += r2 < 2.25f ? 1u : 0u;
+        }
+    };
+
+    bool lost = false;
+    for (uint32_t t = 0; t < tiles; t++) {
+        const uint32_t slot = t % kStageSlots;
+        const bool ok = bar_wait(&st.bar[slot], (t / kStageSlots) & 1u);
+        if (__syncthreads_or(!ok)) {
+            lost = true;
+            break;
+        }
+        const uint32_t* tile = reinterpret_cast<const uint32_t*>(&st.rows[slot][0][0]);
+        const uint32_t k0 = t * kStageRows * 4u + sub;  // this lane's first entry in the tile
+        // four entries per round: indices from shared memory, then all four
+        // gathers, then the arithmetic
+#pragma unroll
+        for (int half = 0; half < kStageRows; half += 4) {
+            uint32_t j[4];
+            bool use[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const uint32_t k = k0 + (uint32_t)(half + r) * 4u;
+                use[r] = k < cnt;
+                j[r] = use[r] ? tile[((half + r) * kBlockParticles + p) * 4u + sub] : i;
+            }
+            uint4 pj[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) pj[r] = use[r] ? __ldg(cur + j[r]) : own;
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                if (use[r]) accumulate(pj[r]);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && t + kStageSlots < tiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tile_load(map, &st.rows[slot][0][0], &st.bar[slot], (int)(first * 4u),
+                      (int)((t + kStageSlots) * kStageRows));
+        }
+    }
+    if (lost) {
+        // record the fault, then let the tiles still in flight land before
+        // the block's shared memory goes away
+        if (threadIdx.x == 0) {
+            atomicCAS(&a.glob->fault, 0u, kFaultTmaTimeout);
+            for (uint32_t t = 0; t < tiles && t < (uint32_t)kStageSlots; t++)
+                bar_wait(&st.bar[t], 0u);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int o = 1; o < kLanes; o <<= 1) {
+        s.ax += __shfl_xor_sync(kFull, s.ax, o);
+        s.ay += __shfl_xor_sync(kFull, s.ay, o);
+        s.az += __shfl_xor_sync(kFull, s.az, o);
+        if (ENERGIES) {
+            float t, e;
+            const float pe = __shfl_xor_sync(kFull, s.pe, o), pl = __shfl_xor_sync(kFull, s.pe_lo, o);
+            two_sum(s.pe, pe, t, e);
+            s.pe = t;
+            s.pe_lo = (s.pe_lo + pl) + e;
+            const float w = __shfl_xor_sync(kFull, s.w, o), wl = __shfl_xor_sync(kFull, s.w_lo, o);
+            two_sum(s.w, w, t, e);
+            s.w = t;
+            s.w_lo = (s.w_lo + wl) + e;
+            s.near += __shfl_xor_sync(kFull, s.near, o);
+        }
+    }
+    return s;
+}
+
+__device__ __forceinline__ float component(const PairSums& s, uint32_t k) {
+    return k == 0 ? s.ax : (k == 1 ? s.ay : s.az);
+}
+
+// Langevin noise for coordinate k of a particle: Philox-4x32-10 (Salmon et
+// al., SC'11) with counter (id, step lo, step hi, 0) and key (seed, "LJV1");
+// uniforms in (0, 1] from 24 bits as the reference's uniform01
+// (lennard_jones.wgsl:175-178); Box-Muller in f32: x and y from the first
+// pair of uniforms (cosine and sine), z from the second (cosine).
+__device__ __forceinline__ float langevin_component(uint32_t id, unsigned long long step,
+                                                   uint32_t seed, uint32_t k) {
+    const uint4 r = philox(id, step, seed);
+    const uint32_t ra = k < 2 ? r.x : r.z, rb = k < 2 ? r.y : r.w;
+    const float ua = __fdiv_rn((float)(ra >> 8) + 1.0f, 16777216.0f);
+    const float ub = __fdiv_rn((float)(rb >> 8) + 1.0f, 16777216.0f);
+    const float radius = sqrtf(-2.0f * logf(ua));
+    const float angle = 6.283185307179586f * ub;
+    return k == 1 ? radius * sinf(angle) : radius * cosf(angle);
+}
+
+// ---- prime (lennard_jones.wgsl:547-553): first forces; the stored velocity
+// becomes half a kick behind the given one ----
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) prime_kernel(Arena a, const __grid_constant__ CUtensorMap map) {
+    count_kernel(a);
+    __shared__ __align__(128) Stage st;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const bool valid = i < a.nslots;
+    const Box& bx = a.boxes[valid ? box_of_slot(a, i) : 0u];
+    const PairSums s = block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, sub, valid,
+                                                             a.cache[a.glob->phase]);
+    if (valid && sub < 3) a.v[sub * a.seg + i] -= (double)component(s, sub) * bx.half_dt;
+}
+
+// ---- one step: begin + force_kick of the reference fused
+// (lennard_jones.wgsl:204-276, 556-574) ----
+// The stored velocity is half a kick behind, so this kernel's force pass
+// applies the previous step's closing half kick and this step's opening half
+// kick together, then drifts: x += v dt (constant energy), or the Langevin
+// A-O-A: x += v dt/2; v = c1 v + c2 xi; x += v dt/2. State updates in f64.
+// The new position goes to the other cache copy (neighbours still read this
+// step's), and the largest squared displacement since the last list build
+// feeds the next step's rebuild decision.
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) step_kernel(Arena a, const __grid_constant__ CUtensorMap map) {
+    count_kernel(a);
+    __shared__ __align__(128) Stage st;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const bool valid = i < a.nslots;
+    const uint32_t phase = a.glob->phase;
+    const uint32_t b = valid ? box_of_slot(a, i) : 0u;
+    const Box& bx = a.boxes[b];
+    const PairSums s =
+        block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, sub, valid, a.cache[phase]);
+    uint32_t enc = 0;
+    float d2 = 0.0f;
+    if (valid && sub < 3) {
+        const size_t q = (size_t)sub * a.seg + i;
+        double x = a.x[q];
+        double v = a.v[q] + (double)component(s, sub) * bx.dt;
+        if (bx.thermostat == 1) {
+            const float xi = langevin_component(a.id[i], a.glob->step, bx.seed, sub);
+            x += v * bx.half_dt;
+            v = bx.c1 * v + bx.c2 * (double)xi;
+            x += v * bx.half_dt;
+        } else {
+            x += v * bx.dt;
+        }
+        x = wrap(x, bx.box[sub]);
+        a.x[q] = x;
+        a.v[q] = v;
+        enc = encode(x, bx.enc[sub]);
+        const uint32_t snap = reinterpret_cast<const uint32_t*>(a.snap + i)[sub];
+        const float d = decode_diff(enc, snap, bx.dec[sub]);
+        d2 = d * d;
+    }
+    const uint32_t e1 = __shfl_down_sync(kFull, enc, 1), e2 = __shfl_down_sync(kFull, enc, 2);
+    const float d21 = __shfl_down_sync(kFull, d2, 1), d22 = __shfl_down_sync(kFull, d2, 2);
+    const bool lead = valid && sub == 0;
+    if (lead) a.cache[phase ^ 1u][i] = make_uint4(enc, e1, e2, 0u);
+    block_max_per_box(a, lead, b, blockIdx.x * kBlockParticles, d2 + d21 + d22);
+    if (tid == 0) a.glob->pending = 1u;
+}
+
+// ---- measure (lennard_jones.wgsl:576-626) ----
+// Per particle: half of each pair energy and virial, neighbours within
+// 1.5 sigma, the velocity at the step (stored velocity plus the closing half
+// kick), kinetic energy and momentum in f64. Each value goes to 32.32 fixed
+// point scaled like the reference and is summed exactly.
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, const __grid_constant__ CUtensorMap map,
+                                                         int canonical) {
+    count_kernel(a);
+    __shared__ __align__(128) Stage st;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const bool valid = i < a.nslots;
+    const uint32_t b = valid ? box_of_slot(a, i) : 0u;
+    const Box& bx = a.boxes[b];
+    const PairSums s = block_pair_sums<SHIFTED_FORCE, true>(st, &map, a, bx, i, sub, valid,
+                                                            a.cache[a.glob->phase]);
+    double vel = 0.0;
+    if (valid && sub < 3) {
+        vel = a.v[(size_t)sub * a.seg + i] + (double)component(s, sub) * bx.half_dt;
+        if (canonical) a.vcanon[(size_t)sub * a.seg + i] = vel;
+    }
+    const double vy = __shfl_down_sync(kFull, vel, 1), vz = __shfl_down_sync(kFull, vel, 2);
+    const bool lead = valid && sub == 0;
+    long long v[kSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (lead) {
+        const double vx = vel;
+        double ke = 0.0;
+        ke += vx * vx;
+        ke += vy * vy;
+        ke += vz * vz;
+        ke *= 0.5;
+        const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
+        v[0] = fixed_raw_f64(ke * es);
+        v[1] = fixed_raw_f32(s.pe * bx.energy_scale) + fixed_raw_f32(s.pe_lo * bx.energy_scale);
+        v[2] = fixed_raw_f32(s.w * bx.energy_scale) + fixed_raw_f32(s.w_lo * bx.energy_scale);
+        v[3] = fixed_raw_f64(vx * ms);
+        v[4] = fixed_raw_f64(vy * ms);
+        v[5] = fixed_raw_f64(vz * ms);
+        v[6] = s.near >= bx.near_count ? (1ll << 32) : 0ll;
+        a.pe_half[2 * i] = s.pe;
+        a.pe_half[2 * i + 1] = s.pe_lo;
+        a.w_half[2 * i] = s.w;
+        a.w_half[2 * i + 1] = s.w_lo;
+        a.vel4[i] = make_float4((float)vx, (float)vy, (float)vz, (float)s.near);
+    }
+    block_sum_slots(a, lead, b, blockIdx.x * kBlockParticles, v);
+}
+
+// ---- FP32 calibration: eight independent FMA chains per thread, so the
+// FMA pipes stay full; 2 flops per FMA ----
+__global__ void __launch_bounds__(kBlock) fp32_peak_kernel(float* out, int iters) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+    const float m = 0.999999f, c = 1e-6f;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = fmaf(x[k], m, c);
+    }
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) t += x[k];
+    if (t == 12345.678f) out[blockIdx.x] = t;  // keeps the chains live
+}
+
+// ---- launchers ----
+static unsigned particle_blocks(const Arena& a) {
+    return blocks_for((uint64_t)a.nslots * kLanes);
+}
+
+cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_force,
+                         cudaStream_t s) {
+    if (shifted_force)
+        prime_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+    else
+        prime_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+    return after_launch();
+}
+
+cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
+                        cudaStream_t s) {
+    if (shifted_force)
+        step_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+    else
+        step_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+    return after_launch();
+}
+
+cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_force,
+                           bool canonical, cudaStream_t s) {
+    if (shifted_force)
+        measure_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map, canonical ? 1 : 0);
+    else
+        measure_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map, canonical ? 1 : 0);
+    return after_launch();
+}
+
+cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s) {
+    fp32_peak_kernel<<<blocks, kBlock, 0, s>>>(out, iters);
+    return after_launch();
+}
+
+}  // namespace vlj

@@ -1,0 +1,461 @@
+// CUDA kernels of the cell grid and the Verlet lists, sm_100a.
+//
+// A step starts with `decide` (one block: flip the position copy, pick the
+// boxes that rebuild). The rebuild chain that follows -- bin, scan, scatter,
+// per-cell order with the optional reorder, copy back, pack, list build --
+// sits under a conditional graph node, so it runs only on steps where some
+// box crossed the skin / 2 trigger; launched directly, each kernel returns at
+// once when nothing rebuilds. Reference kernels are cited at each kernel.
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "vlj_device.cuh"
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launches() { return g_launches.load(); }
+
+cudaError_t after_launch(unsigned n) {
+    g_launches += n;
+    return cudaGetLastError();
+}
+
+// ---- encode positions into the current cache copy ----
+__global__ void encode_kernel(Arena a) {
+    count_kernel(a);
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[box_of_slot(a, i)];
+    uint4 w;
+    w.x = encode(a.x[i], bx.enc[0]);
+    w.y = encode(a.x[a.seg + i], bx.enc[1]);
+    w.z = encode(a.x[2 * a.seg + i], bx.enc[2]);
+    w.w = 0u;
+    a.cache[a.glob->phase][i] = w;
+}
+
+// ---- decide (lennard_jones.wgsl:281-307) ----
+// One block. Finishes the previous step's bookkeeping (flip the position
+// copy, advance the step counter), then per box: rebuild when something moved
+// more than skin / 2 since the last build, or never built; reorder on every
+// reorder_every-th rebuild (counted before the increment, as the reference).
+template <bool SET_CONDITION>
+__global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
+    count_kernel(a);
+    __shared__ int s_any;
+    Global* g = a.glob;
+    if (threadIdx.x == 0) {
+        s_any = 0;
+        if (g->pending) {
+            g->phase ^= 1u;
+            g->step += 1ull;
+            g->pending = 0u;
+        }
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < a.nboxes; b += blockDim.x) {
+        Control& c = a.ctrl[b];
+        const Box& bx = a.boxes[b];
+        float moved = __uint_as_float(c.max_disp);
+        c.max_disp = 0u;
+        bool rebuild = moved > bx.half_skin2 || c.built == 0u || c.forced != 0u;
+        c.forced = 0u;
+        c.rebuild = rebuild ? 1u : 0u;
+        if (rebuild) {
+            c.reorder = (c.rebuilds % bx.reorder_every == 0u) ? 1u : 0u;
+            c.rebuilds += 1u;
+            c.built = 1u;
+            s_any = 1;
+        } else {
+            c.reorder = 0u;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g->any = (uint32_t)s_any;
+        if (SET_CONDITION) cudaGraphSetConditional(handle, (unsigned)s_any);
+    }
+}
+
+// ---- bin (grid.wgsl:11-38): cell of each slot from its f32 position ----
+__global__ void bin_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    uint32_t b = box_of_slot(a, i);
+    if (!rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    int32_t c[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float hi = (float)a.x[k * a.seg + i];
+        int32_t v = (int32_t)floorf(__fdiv_rn(hi, bx.cell_size_f[k]));
+        int32_t m = (int32_t)bx.cells[k] - 1;
+        c[k] = v < 0 ? 0 : (v > m ? m : v);
+    }
+    uint32_t cell =
+        bx.cell_base + ((uint32_t)c[2] * bx.cells[1] + (uint32_t)c[1]) * bx.cells[0] + (uint32_t)c[0];
+    a.cell_of_slot[i] = cell;
+    atomicAdd(&a.count[cell], 1u);
+}
+
+// ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
+// the counts offset by the box's first slot; counts become zeroed cursors.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t b = blockIdx.x;
+    if (b >= a.nboxes || !rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    __shared__ uint32_t s_carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_carry = bx.first;
+    __syncthreads();
+    const uint32_t total = bx.total_cells, base = bx.cell_base;
+    for (uint32_t tile = 0; tile < total; tile += kScanThreads * kScanPer) {
+        uint32_t v[kScanPer];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) {
+            uint32_t c = tile + threadIdx.x * kScanPer + q;
+            v[q] = c < total ? a.count[base + c] : 0u;
+            sum += v[q];
+        }
+        // inclusive scan of the per-thread sums
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += t;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        uint32_t before = s_carry + (warp ? s_warp[warp - 1] : 0u) + incl - sum;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) {
+            uint32_t c = tile + threadIdx.x * kScanPer + q;
+            if (c < total) {
+                a.cell_start[base + c] = before;
+                a.count[base + c] = 0u;
+            }
+            before += v[q];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += s_warp[kScanThreads / 32 - 1];
+        __syncthreads();
+    }
+}
+
+// ---- scatter (grid.wgsl:119-127): slot into its cell's next free place ----
+__global__ void scatter_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    if (!rebuilding(a, box_of_slot(a, i))) return;
+    uint32_t c = a.cell_of_slot[i];
+    a.sorted[a.cell_start[c] + atomicAdd(&a.count[c], 1u)] = i;
+}
+
+// ---- per-cell order (grid.wgsl:129-148) ----
+// One warp per cell: each slot's rank is the number of smaller slots in the
+// cell, so the cell ends up sorted by slot index whatever order the scatter's
+// atomics produced. With reorder, every particle is also copied to the slot
+// it takes in cell order (lennard_jones.wgsl:419-433).
+constexpr int kSortRegs = 8;  // cells up to 256 particles rank in registers
+
+__device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, uint32_t to,
+                                                uint32_t cell) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        a.sx[k * a.seg + to] = a.x[k * a.seg + from];
+        a.sv[k * a.seg + to] = a.v[k * a.seg + from];
+    }
+    a.sid[to] = a.id[from];
+    a.scell[to] = cell;
+}
+
+__global__ void sort_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cell >= a.ncells) return;
+    uint32_t b = box_of_cell(a, cell);
+    if (!rebuilding(a, b)) return;
+    const bool reorder = a.ctrl[b].reorder != 0u;
+    const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
+    const uint32_t m = end - start;
+    if (lane == 0) a.count[cell] = 0u;
+    if (m <= 32u * kSortRegs) {
+        uint32_t key[kSortRegs], rank[kSortRegs];
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
+            rank[r] = 0;
+        }
+        for (int rr = 0; rr < kSortRegs; rr++) {
+            if ((uint32_t)rr * 32u >= m) break;
+            for (int src = 0; src < 32; src++) {
+                uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
+#pragma unroll
+                for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            if (t < m) {
+                a.sorted[start + rank[r]] = key[r];
+                if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
+            }
+        }
+    } else if (lane == 0) {
+        // insertion sort, as the reference, for improbably full cells
+        for (uint32_t s = start + 1; s < end; s++) {
+            uint32_t key = a.sorted[s];
+            uint32_t t = s;
+            while (t > start && a.sorted[t - 1] > key) {
+                a.sorted[t] = a.sorted[t - 1];
+                t -= 1;
+            }
+            a.sorted[t] = key;
+        }
+        if (reorder)
+            for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
+    }
+}
+
+// ---- reorder copy back (lennard_jones.wgsl:435-452) ----
+__global__ void reorder_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nslots) return;
+    uint32_t b = box_of_slot(a, s);
+    if (!rebuilding(a, b) || !a.ctrl[b].reorder) return;
+    const Box& bx = a.boxes[b];
+    uint4 w;
+    double xs[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        xs[k] = a.sx[k * a.seg + s];
+        a.x[k * a.seg + s] = xs[k];
+        a.v[k * a.seg + s] = a.sv[k * a.seg + s];
+    }
+    a.id[s] = a.sid[s];
+    a.cell_of_slot[s] = a.scell[s];
+    a.sorted[s] = s;
+    w.x = encode(xs[0], bx.enc[0]);
+    w.y = encode(xs[1], bx.enc[1]);
+    w.z = encode(xs[2], bx.enc[2]);
+    w.w = 0u;
+    a.cache[a.glob->phase][s] = w;
+}
+
+// ---- the reference's packed positions for the list build
+// (lennard_jones.wgsl:154-164; hi/lo as Df64::from_f64, lennard_jones.rs:476-489)
+__global__ void pack_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nslots) return;
+    if (!rebuilding(a, box_of_slot(a, s))) return;
+    float h[3], l[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double x = a.x[k * a.seg + s];
+        h[k] = (float)x;
+        l[k] = (float)(x - (double)h[k]);
+    }
+    float3 hi = make_float3(h[0], h[1], h[2]);
+    float3 lo = make_float3(l[0], l[1], l[2]);
+    a.ref[s] = make_float4(h[0], h[1], h[2], __uint_as_float(pack_lo(hi, lo)));
+    a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
+}
+
+// ---- Verlet list build (lennard_jones.wgsl:454-499) ----
+// Everything within cutoff + skin, cells in the order dz, dy, dx = -1..1 with
+// periodic wrap, then each cell in sorted order; one thread per particle.
+// Acceptance is the reference's f32 test on packed positions, operation for
+// operation, so the list is the reference's entry for entry. Two cheaper,
+// exact shortcuts keep that order:
+//  - a neighbour cell whose box lies farther from the particle than the list
+//    radius (plus a margin) cannot hold a list entry and is skipped;
+//  - a test on the 32-bit encoded positions settles every candidate farther
+//    than sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in): the
+//    two radii bracket list_r2 by more than the reference's f32 separations
+//    and the encoded ones can differ, so only candidates in the thin shell
+//    between them need the reference's own arithmetic.
+struct RefTest {
+    float xh[3], xl[3], side[3], inv[3], list_r2;
+    const float* q510;
+    // the reference's predicate for a packed neighbour position
+    __device__ __forceinline__ bool operator()(const float4 pj) const {
+        const uint32_t bits = __float_as_uint(pj.w);
+        const float ph[3] = {pj.x, pj.y, pj.z};
+        float d[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float lo = __fmul_rn(q510[(bits >> (9u * k)) & 511u], last_bit(ph[k]));
+            const float e = __fadd_rn(__fsub_rn(ph[k], xh[k]), __fsub_rn(lo, xl[k]));
+            d[k] = nearest_ref_fast(e, side[k], inv[k]);
+        }
+        const float r2 =
+            __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2]));
+        return r2 < list_r2;
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) build_list_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
+    for (int t = threadIdx.x; t < 512; t += blockDim.x)
+        s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const uint32_t b = box_of_slot(a, i);
+    if (!rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    const uint4* __restrict__ cur = a.cache[a.glob->phase];
+    const uint4 own_enc = cur[i];
+    const float4 own = a.ref[i];
+    const float4 own_lo = a.ref_lo[i];
+    RefTest test;
+    test.xh[0] = own.x, test.xh[1] = own.y, test.xh[2] = own.z;
+    test.xl[0] = own_lo.x, test.xl[1] = own_lo.y, test.xl[2] = own_lo.z;
+    for (int k = 0; k < 3; k++) {
+        test.side[k] = bx.box_f[k];
+        test.inv[k] = bx.inv_box_f[k];
+    }
+    test.list_r2 = bx.list_r2;
+    test.q510 = s_q510;
+    const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
+    const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};
+    const int32_t ci = (int32_t)(a.cell_of_slot[i] - bx.cell_base);
+    const int32_t c[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+    // squared distance from the particle to the faces of its cell, per axis
+    // and side, less a margin for the f32 binning: a neighbour cell farther
+    // than the list radius by these bounds holds no list entry
+    float gap2[3][2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float lo = (float)c[k] * bx.cell_size_f[k];
+        const float below = fmaxf(test.xh[k] - lo - 1e-3f, 0.0f);
+        const float above = fmaxf(lo + bx.cell_size_f[k] - test.xh[k] - 1e-3f, 0.0f);
+        gap2[k][0] = below * below;
+        gap2[k][1] = above * above;
+    }
+    const uint32_t cap = bx.capacity;
+    const float pre_r2 = bx.prefilter_r2, acc_r2 = bx.accept_r2;
+    uint32_t found = 0;
+    auto take = [&](uint32_t j, uint4 pe) {
+        const float r2e = encoded_r2(pe, own_enc, dec);
+        bool in;
+        if (r2e < acc_r2)
+            in = true;
+        else if (r2e < pre_r2)
+            in = test(a.ref[j]);
+        else
+            return;
+        if (in) {
+            if (found < cap) a.list[((size_t)(found >> 2) * a.seg + i) * 4u + (found & 3u)] = j;
+            found += 1;
+        }
+    };
+    for (int32_t dz = -1; dz <= 1; dz++) {
+        const float gz = dz == 0 ? 0.0f : gap2[2][dz > 0];
+        if (gz > pre_r2) continue;
+        int32_t uz = c[2] + dz;
+        uz = uz < 0 ? uz + n[2] : (uz >= n[2] ? uz - n[2] : uz);
+        for (int32_t dy = -1; dy <= 1; dy++) {
+            const float gzy = gz + (dy == 0 ? 0.0f : gap2[1][dy > 0]);
+            if (gzy > pre_r2) continue;
+            int32_t uy = c[1] + dy;
+            uy = uy < 0 ? uy + n[1] : (uy >= n[1] ? uy - n[1] : uy);
+            const uint32_t row = bx.cell_base + ((uint32_t)uz * (uint32_t)n[1] + (uint32_t)uy) * (uint32_t)n[0];
+            for (int32_t dx = -1; dx <= 1; dx++) {
+                if (gzy + (dx == 0 ? 0.0f : gap2[0][dx > 0]) > pre_r2) continue;
+                int32_t ux = c[0] + dx;
+                ux = ux < 0 ? ux + n[0] : (ux >= n[0] ? ux - n[0] : ux);
+                const uint32_t cell = row + (uint32_t)ux;
+                const uint32_t end = a.cell_start[cell + 1];
+                uint32_t t = a.cell_start[cell];
+                // two candidates per round, both gathers in flight together
+                for (; t + 1 < end; t += 2) {
+                    const uint32_t j0 = a.sorted[t], j1 = a.sorted[t + 1];
+                    const uint4 p0 = __ldg(cur + j0), p1 = __ldg(cur + j1);
+                    if (j0 != i) take(j0, p0);
+                    if (j1 != i) take(j1, p1);
+                }
+                if (t < end) {
+                    const uint32_t j0 = a.sorted[t];
+                    if (j0 != i) take(j0, __ldg(cur + j0));
+                }
+            }
+        }
+    }
+    const uint32_t kept = found < cap ? found : cap;
+    a.list_count[i] = kept;
+    if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
+    a.snap[i] = own_enc;
+    // the longest list, one atomic per warp when the whole warp is here
+    if (__activemask() == 0xffffffffu) {
+        uint32_t m = kept;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31u) == 0) atomicMax(&a.glob->max_count, m);
+    } else {
+        atomicMax(&a.glob->max_count, kept);
+    }
+}
+
+// ---- launchers ----
+cudaError_t launch_encode(const Arena& a, cudaStream_t s) {
+    encode_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle) {
+    if (cond_handle)
+        decide_kernel<true><<<1, kBlock, 0, s>>>(a, (cudaGraphConditionalHandle)cond_handle);
+    else
+        decide_kernel<false><<<1, kBlock, 0, s>>>(a, (cudaGraphConditionalHandle)0);
+    return after_launch();
+}
+
+cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
+    const unsigned slots = blocks_for(a.nslots);
+    bin_kernel<<<slots, kBlock, 0, s>>>(a);
+    scan_kernel<<<a.nboxes, kScanThreads, 0, s>>>(a);
+    scatter_kernel<<<slots, kBlock, 0, s>>>(a);
+    sort_kernel<<<blocks_for((uint64_t)a.ncells * 32u), kBlock, 0, s>>>(a);
+    reorder_kernel<<<slots, kBlock, 0, s>>>(a);
+    pack_kernel<<<slots, kBlock, 0, s>>>(a);
+    build_list_kernel<<<slots, kBlock, 0, s>>>(a);
+    return after_launch(7);
+}
+
+}  // namespace vlj

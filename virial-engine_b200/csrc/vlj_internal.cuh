@@ -18,13 +18,18 @@
 //             the hi part's last bit in w) and ref_lo (the full f32 lo part).
 //             The list build uses exactly the reference's f32 predicate on
 //             these, so lists match it bit for bit.
-//   list      u32, transposed: entry k of slot i at list[k * seg + i];
-//             counts in list_count[i].
+//   list      u32 slot indices, interleaved by four: entry k of slot i at
+//             list[((k / 4) * seg + i) * 4 + k % 4], counts in list_count[i].
+//             A row of the list (four entries of every slot) is 16 B per
+//             slot, so the four lanes that serve a particle read one 16 B
+//             word and a warp reads one contiguous 128 B line; the force
+//             kernels stage row tiles into shared memory with TMA.
 //   cells     per cell: count (atomic cursor) and start. Boxes own contiguous
 //             runs of slots and cells, so one start array of ncells + 1 entries
 //             serves every box: box b's last cell ends where box b + 1 begins.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -32,6 +37,10 @@ namespace vlj {
 
 constexpr int kBlock = 256;
 constexpr int kSlots = 8;  // measurement accumulators per box
+constexpr int kLanes = 4;  // threads per particle in the force kernels
+constexpr int kBlockParticles = kBlock / kLanes;
+constexpr int kStageRows = 8;   // list rows (32 entries per particle) per TMA tile
+constexpr int kStageSlots = 3;  // tiles in flight per block
 // measurement slots: 0 kinetic, 1 potential, 2 virial, 3-5 momentum,
 // 6 condensed count, 7 unused (lennard_jones.wgsl:576-626)
 
@@ -51,6 +60,7 @@ struct Box {
     float bin_width;
     float inv_box_f[3];  // 1 / box_f, for nearest_ref_fast
     float prefilter_r2;  // list_r2 widened past any encoding difference
+    float accept_r2;     // list_r2 narrowed past any encoding difference
     uint32_t cells[3];
     uint32_t total_cells;
     uint32_t cell_base;  // first cell of this box
@@ -86,7 +96,12 @@ struct Global {
     uint32_t fault;      // first error a kernel recorded (0 none)
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
+    uint32_t max_count;          // longest list built so far (rows the force kernels stage)
+    uint32_t pad;
 };
+
+// Fault codes in Global::fault (the first one recorded wins).
+constexpr uint32_t kFaultTmaTimeout = 1;  // a TMA tile never arrived
 
 // Every pointer a kernel needs; passed by value (it sits in the constant
 // bank), so captured graphs see fixed pointers and read the mutable state
@@ -202,22 +217,6 @@ __device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, ui
     return make_uint4(c0, c1, c2, c3);
 }
 
-// Three gaussians: uniforms in (0, 1] from 24 bits (as the reference's
-// uniform01, lennard_jones.wgsl:175-178), Box-Muller in f32.
-__device__ __forceinline__ float3 langevin_noise(uint32_t id, unsigned long long step,
-                                                 uint32_t seed) {
-    uint4 r = philox(id, step, seed);
-    float u0 = __fdiv_rn((float)(r.x >> 8) + 1.0f, 16777216.0f);
-    float u1 = __fdiv_rn((float)(r.y >> 8) + 1.0f, 16777216.0f);
-    float u2 = __fdiv_rn((float)(r.z >> 8) + 1.0f, 16777216.0f);
-    float u3 = __fdiv_rn((float)(r.w >> 8) + 1.0f, 16777216.0f);
-    float ra = sqrtf(-2.0f * logf(u0));
-    float aa = 6.283185307179586f * u1;
-    float rb = sqrtf(-2.0f * logf(u2));
-    float ab = 6.283185307179586f * u3;
-    return make_float3(ra * cosf(aa), ra * sinf(aa), rb * cosf(ab));
-}
-
 // r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545). The
 // reciprocal and square root are the hardware approximations (about 1 ulp),
 // well inside the f32 pair arithmetic's own error.
@@ -238,11 +237,17 @@ __device__ __forceinline__ void lj_pair(float r2, const Box& b, float& rf, float
 // |F| / r of a pair at r2 < rc2: the factor that multiplies the separation.
 template <bool SHIFTED_FORCE>
 __device__ __forceinline__ float lj_force_over_r2(float r2, float force_shift) {
-    float inv2 = __fdividef(1.0f, r2);
-    float s6 = inv2 * inv2 * inv2;
-    float rf = 24.0f * s6 * (2.0f * s6 - 1.0f);
-    if (SHIFTED_FORCE) rf -= r2 * rsqrtf(r2) * force_shift;
-    return rf * inv2;
+    if (SHIFTED_FORCE) {
+        // one reciprocal square root gives both 1/r^2 and r
+        const float inv_r = rsqrtf(r2);
+        const float inv2 = inv_r * inv_r;
+        const float s6 = inv2 * inv2 * inv2;
+        const float rf = 24.0f * s6 * (2.0f * s6 - 1.0f) - r2 * inv_r * force_shift;
+        return rf * inv2;
+    }
+    const float inv2 = __fdividef(1.0f, r2);
+    const float s6 = inv2 * inv2 * inv2;
+    return 24.0f * s6 * (2.0f * s6 - 1.0f) * inv2;
 }
 
 // The reference's nearest image d - side * round(d / side) with the IEEE
@@ -273,9 +278,15 @@ __device__ __forceinline__ float encoded_r2(uint4 a, uint4 b, const float dec[3]
 cudaError_t launch_encode(const Arena& a, cudaStream_t s);
 cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle);
 cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
-cudaError_t launch_prime(const Arena& a, bool shifted_force, cudaStream_t s);
-cudaError_t launch_step(const Arena& a, bool shifted_force, cudaStream_t s);
-cudaError_t launch_measure(const Arena& a, bool shifted_force, bool canonical, cudaStream_t s);
+// The force kernels read list rows through `list_map`: a 2D TMA tensor map
+// over the list (inner dimension 4 * seg u32, outer one row per four
+// entries) whose box is kStageRows rows of kBlockParticles slots.
+cudaError_t launch_prime(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
+                         cudaStream_t s);
+cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
+                        cudaStream_t s);
+cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
+                           bool canonical, cudaStream_t s);
 cudaError_t launch_profile(const Arena& a, bool shifted_force, cudaStream_t s);
 cudaError_t launch_heat_current(const Arena& a, bool shifted_force, cudaStream_t s);
 cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s);

@@ -1,6 +1,8 @@
 // The simulation object behind the opaque vlj_sim handle.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -36,6 +38,7 @@ struct vlj_sim {
     bool shifted_force = false;
     vlj::Box box{};
     vlj::Arena arena{};
+    CUtensorMap list_map;  // list rows for the force kernels' TMA tiles
     std::vector<void*> allocations;
     uint64_t steps = 0;
     // measurement read-back ring
@@ -67,5 +70,7 @@ struct vlj_sim {
 
 namespace vlj {
 vlj_status sim_allocate(vlj_sim* s, void* stream);
+vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out);
+vlj_status check_fault(vlj_sim* s);
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
 }  // namespace vlj

@@ -26,11 +26,15 @@ def main():
     ap.add_argument("--truncated", action="store_true", help="truncated-shifted, not force-shifted")
     ap.add_argument("--nve", action="store_true", help="constant energy instead of Langevin")
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="enqueue steps as direct launches (profilers see each kernel)")
     args = ap.parse_args()
     p, box = vl.lattice_fcc(args.cells, args.density, args.temperature, args.seed)
     thermostat = None if args.nve else vl.Langevin(args.temperature, 1.0, args.seed)
     sim = vl.LennardJones(p, vl.Settings([box] * 3, dt=args.dt, thermostat=thermostat,
                                          shifted_force=not args.truncated))
+    if args.no_graphs:
+        sim.set_graphs(False)
     m = sim.measure_now()
     print(f"{len(p)} particles, box {box:.4f}: E {m.energy():.6f} P {m.pressure():.6f}")
     t0 = time.perf_counter()
