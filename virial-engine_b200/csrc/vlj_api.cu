@@ -116,6 +116,8 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
     double list_r = std::sqrt((double)b.list_r2);
     b.prefilter_r2 = (float)((list_r + margin) * (list_r + margin));
     b.accept_r2 = (float)((list_r - margin) * (list_r - margin));
+    // a particle binned into a cell lies within 1e-3 of the cell's box
+    b.reach_r2 = (float)((list_r + margin + 1e-3) * (list_r + margin + 1e-3));
     for (int k = 0; k < 3; k++) b.inv_box_f[k] = 1.0f / b.box_f[k];
     b.dt = dt;
     b.half_dt = 0.5 * dt;
@@ -690,10 +692,12 @@ vlj_status vlj_debug_launches(uint64_t* n) {
 // ---- allocation and step enqueue (shared with the graph path) ----
 namespace vlj {
 
-// The 2D tensor map the force kernels stage list rows through: inner
-// dimension 4 * seg u32 (four entries of every slot), outer one row per four
-// list entries; box kStageRows rows of kBlockParticles slots. Row stride
-// 16 * seg bytes (seg is a multiple of 16, so 16-byte aligned as TMA needs).
+// The 2D tensor map the force kernels stage list rows through: the list seen
+// as u64 pairs of entries, inner dimension 2 * seg (a row holds four entries
+// of every slot), outer one row per four list entries; box kTileRows rows of
+// kForceThreads slots (2 * kForceThreads <= 256 elements, TMA's box limit).
+// Row stride 16 * seg bytes (seg is a multiple of 16, so 16-byte aligned as
+// TMA needs).
 vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -704,11 +708,11 @@ vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out) {
             return fail(VLJ_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
-    const cuuint64_t dims[2] = {(cuuint64_t)a.seg * 4u, (cuuint64_t)rows};
+    const cuuint64_t dims[2] = {(cuuint64_t)a.seg * 2u, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)a.seg * 16u};
-    const cuuint32_t box[2] = {(cuuint32_t)kBlockParticles * 4u, (cuuint32_t)kStageRows};
+    const cuuint32_t box[2] = {(cuuint32_t)kForceThreads * 2u, (cuuint32_t)kTileRows};
     const cuuint32_t estrides[2] = {1u, 1u};
-    CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, a.list, dims, strides, box, estrides,
+    CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, a.list, dims, strides, box, estrides,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(VLJ_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);

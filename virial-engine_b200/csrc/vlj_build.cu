@@ -1,0 +1,178 @@
+// Verlet list build for sm_100a (lennard_jones.wgsl:454-499).
+//
+// Each particle's list holds everything within cutoff + skin, in the
+// reference's order: the 27 cells dz, dy, dx = -1..1 (periodic wrap), each in
+// its sorted order, skipping the particle itself. Acceptance is the
+// reference's f32 test on packed positions, operation for operation, so the
+// lists are the reference's entry for entry.
+//
+// One warp serves one home cell: up to 32 home particles, one per lane. For
+// each neighbour cell in stencil order the warp copies the cell's candidates
+// (slot and encoded position) into shared memory once, then every lane tests
+// its home particle against each candidate in turn -- the same candidates in
+// the same order for all lanes, so the warp never diverges on the stream and
+// the inner loop reads only shared memory. A test on the 32-bit encoded
+// positions settles every candidate farther than sqrt(prefilter_r2) (out) or
+// nearer than sqrt(accept_r2) (in); the two radii bracket list_r2 by more
+// than the reference's f32 separations and the encoded ones can differ, so
+// only candidates in the thin shell between them need the reference's own
+// arithmetic.
+#include <cuda_runtime.h>
+
+#include "vlj_device.cuh"
+#include "vlj_internal.cuh"
+
+namespace vlj {
+
+constexpr int kBuildWarps = 8;  // home cells per block
+
+// The reference's predicate for slots i and j: nearest((pj.hi - xh) +
+// (unpack(pj) - xl)), squared length < list_r2, in f32 as written
+// (lennard_jones.wgsl:482-484). Loads its operands itself: it runs only for
+// candidates in the thin shell around the list radius.
+__device__ __noinline__ bool ref_test(const Arena& a, const Box& bx, uint32_t i, uint32_t j,
+                                      const float* q510) {
+    const float4 own = a.ref[i], own_lo = a.ref_lo[i], pj = a.ref[j];
+    const float xh[3] = {own.x, own.y, own.z}, xl[3] = {own_lo.x, own_lo.y, own_lo.z};
+    const float ph[3] = {pj.x, pj.y, pj.z};
+    const uint32_t bits = __float_as_uint(pj.w);
+    float d[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float lo = __fmul_rn(q510[(bits >> (9u * k)) & 511u], last_bit(ph[k]));
+        const float e = __fadd_rn(__fsub_rn(ph[k], xh[k]), __fsub_rn(lo, xl[k]));
+        d[k] = nearest_ref_fast(e, bx.box_f[k], bx.inv_box_f[k]);
+    }
+    const float r2 =
+        __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2]));
+    return r2 < bx.list_r2;
+}
+
+__global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a) {
+    count_kernel(a);
+    if (!a.glob->any) return;
+    __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
+    __shared__ uint32_t s_j[kBuildWarps][32];
+    __shared__ uint4 s_enc[kBuildWarps][32];
+    for (int t = threadIdx.x; t < 512; t += blockDim.x)
+        s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t cell = blockIdx.x * kBuildWarps + warp;
+    if (cell >= a.ncells) return;  // whole warps leave together
+    const uint32_t b = box_of_cell(a, cell);
+    if (!rebuilding(a, b)) return;
+    const Box& bx = a.boxes[b];
+    const uint4* __restrict__ cur = a.cache[a.glob->phase];
+    const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
+    const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};
+    const int32_t ci = (int32_t)(cell - bx.cell_base);
+    const int32_t c[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+    const uint32_t cap = bx.capacity;
+    const float pre_r2 = bx.prefilter_r2, acc_r2 = bx.accept_r2;
+    // The home cell as an interval of encoded coordinates per axis, for the
+    // staging filter: a candidate farther than reach_r2 from the whole home
+    // cell cannot be in any home particle's list.
+    uint32_t home_lo[3], home_w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        home_lo[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)c[k] * (double)bx.cell_size_f[k] * bx.enc[k]);
+        home_w[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)bx.cell_size_f[k] * bx.enc[k]);
+    }
+    const float reach_r2 = bx.reach_r2;
+    const size_t row_stride = (size_t)a.seg * 4u;
+    const unsigned below = (1u << lane) - 1u;
+    uint32_t longest = 0;
+    const uint32_t hbeg = a.cell_start[cell], hend = a.cell_start[cell + 1];
+    for (uint32_t h0 = hbeg; h0 < hend; h0 += 32) {
+        const bool home = h0 + lane < hend;
+        const uint32_t i = home ? a.sorted[h0 + lane] : 0u;
+        const uint4 own_enc = home ? cur[i] : make_uint4(0u, 0u, 0u, 0u);
+        uint32_t found = 0;
+        // where the next entry goes: row (found / 4), column (found % 4)
+        uint32_t* wrow = a.list + (size_t)i * 4u;
+        uint32_t wcol = 0;
+        for (int32_t dz = -1; dz <= 1; dz++) {
+            int32_t uz = c[2] + dz;
+            uz = uz < 0 ? uz + n[2] : (uz >= n[2] ? uz - n[2] : uz);
+            for (int32_t dy = -1; dy <= 1; dy++) {
+                int32_t uy = c[1] + dy;
+                uy = uy < 0 ? uy + n[1] : (uy >= n[1] ? uy - n[1] : uy);
+                const uint32_t row =
+                    bx.cell_base + ((uint32_t)uz * (uint32_t)n[1] + (uint32_t)uy) * (uint32_t)n[0];
+                for (int32_t dx = -1; dx <= 1; dx++) {
+                    int32_t ux = c[0] + dx;
+                    ux = ux < 0 ? ux + n[0] : (ux >= n[0] ? ux - n[0] : ux);
+                    const uint32_t nc = row + (uint32_t)ux;
+                    const uint32_t nend = a.cell_start[nc + 1];
+                    for (uint32_t c0 = a.cell_start[nc]; c0 < nend; c0 += 32) {
+                        // stage up to 32 candidates of this cell, keeping (in
+                        // order) those within reach of the home cell
+                        uint32_t j = 0;
+                        uint4 pe = make_uint4(0u, 0u, 0u, 0u);
+                        bool keep = false;
+                        if (c0 + lane < nend) {
+                            j = a.sorted[c0 + lane];
+                            pe = __ldg(cur + j);
+                            float g2 = 0.0f;
+#pragma unroll
+                            for (int k = 0; k < 3; k++) {
+                                // periodic gap between the candidate and the
+                                // interval [lo, lo + w): above it, or below it
+                                // around the box, whichever is shorter
+                                const uint32_t w = k == 0 ? pe.x : (k == 1 ? pe.y : pe.z);
+                                const uint32_t off = w - home_lo[k];
+                                const uint32_t gap =
+                                    off < home_w[k] ? 0u : min(off - home_w[k], 0u - off);
+                                const float g = (float)gap * dec[k];
+                                g2 += g * g;
+                            }
+                            keep = g2 < reach_r2;
+                        }
+                        const unsigned kept_mask = __ballot_sync(0xffffffffu, keep);
+                        if (keep) {
+                            const uint32_t at = (uint32_t)__popc(kept_mask & below);
+                            s_j[warp][at] = j;
+                            s_enc[warp][at] = pe;
+                        }
+                        __syncwarp();
+                        const uint32_t m = (uint32_t)__popc(kept_mask);
+                        for (uint32_t q = 0; q < m; q++) {
+                            const uint32_t jq = s_j[warp][q];
+                            const float r2e = encoded_r2(s_enc[warp][q], own_enc, dec);
+                            bool in = r2e < acc_r2;
+                            if (!in && r2e < pre_r2 && home && jq != i) in = ref_test(a, bx, i, jq, s_q510);
+                            if (in && home && jq != i) {
+                                if (found < cap) wrow[wcol] = jq;
+                                found += 1;
+                                wcol += 1;
+                                if (wcol == 4u) {
+                                    wcol = 0;
+                                    wrow += row_stride;
+                                }
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        if (home) {
+            const uint32_t kept = found < cap ? found : cap;
+            a.list_count[i] = kept;
+            if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
+            a.snap[i] = own_enc;
+            longest = max(longest, kept);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+    if (lane == 0 && longest) atomicMax(&a.glob->max_count, longest);
+}
+
+cudaError_t launch_build_list(const Arena& a, cudaStream_t s) {
+    build_list_kernel<<<blocks_for(a.ncells, kBuildWarps), kBuildWarps * 32, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace vlj

@@ -13,6 +13,7 @@ inline unsigned blocks_for(uint64_t n, int threads = kBlock) {
     return b ? (unsigned)b : 1u;
 }
 cudaError_t after_launch(unsigned n = 1);
+cudaError_t launch_build_list(const Arena& a, cudaStream_t s);  // vlj_build.cu
 
 __device__ __forceinline__ uint32_t box_of_slot(const Arena& a, uint32_t slot) {
     return a.box_of_slot ? a.box_of_slot[slot] : 0u;

@@ -1,15 +1,14 @@
 // CUDA kernels of the pair forces, the integrator and the measurements,
 // sm_100a.
 //
-// Four lanes of a warp serve one particle. A block serves 64 consecutive
-// slots; their Verlet-list rows (16 B per slot per row, four entries) stream
-// from HBM into shared memory as TMA tiles of 8 rows x 64 slots, three tiles
-// in flight per block, so the list -- most of the step's HBM traffic -- moves
-// asynchronously while the lanes work. Each lane takes one entry of every row
-// (every fourth list entry), gathers the neighbour's encoded position through
-// L1, and the four lanes' sums are combined by warp shuffles in a fixed
-// pattern, so every rerun adds in the same order. Lanes 0, 1 and 2 then
-// update the x, y and z coordinate. Reference kernels are cited at each kernel.
+// One thread per particle, 128 per block. The block's Verlet-list rows (a
+// row is four entries of a particle, 16 B) stream from HBM into shared memory
+// as TMA tiles of 4 rows x 128 particles, three tiles in flight per block, so
+// the list -- most of the step's HBM traffic -- moves asynchronously while
+// the threads work. Each thread reads one whole row per iteration (one 16 B
+// shared-memory load, conflict-free across the warp), issues the four
+// neighbour gathers through L1 together, then does the four pairs' arithmetic.
+// Reference kernels are cited at each kernel.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -18,8 +17,7 @@
 
 namespace vlj {
 
-constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kTileBytes = kStageRows * kBlockParticles * 16u;
+constexpr uint32_t kTileBytes = kTileRows * kForceThreads * 16u;
 constexpr unsigned long long kWaitLimitNs = 500000000ull;  // 0.5 s per TMA tile
 
 struct PairSums {
@@ -31,8 +29,8 @@ struct PairSums {
 
 // Shared memory of a force-kernel block: the tile ring and its barriers.
 struct Stage {
-    uint4 rows[kStageSlots][kStageRows][kBlockParticles];
-    unsigned long long bar[kStageSlots];
+    uint4 rows[kTileSlots][kTileRows][kForceThreads];
+    unsigned long long bar[kTileSlots];
 };
 
 // ---- TMA and mbarrier primitives (PTX, sm_90+) ----
@@ -49,8 +47,9 @@ __device__ __forceinline__ void init_fence() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// One tile: rows [y, y + kStageRows) of slots [x / 4, x / 4 + 64). Rows and
-// slots past the list's end arrive as zeros. No multicast.
+// One tile: rows [y, y + kTileRows) of the block's particles (x = first
+// particle * 2 u64 elements). Rows and particles past the list's end arrive
+// as zeros. No multicast.
 __device__ __forceinline__ void tile_load(const CUtensorMap* map, void* dst, unsigned long long* bar,
                                           int x, int y) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
@@ -90,29 +89,26 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
 // Separations come from the 32-bit box fractions: the wrapped integer
 // difference is the nearest image. The force factor is the same expression
 // in every pass, so the step, the first forces and the measurement agree to
-// the bit. With ENERGIES each lane also sums its halves of pair energy and
-// virial as unevaluated f32 pairs (as the reference sums them in
+// the bit. With ENERGIES the particle's halves of pair energy and virial are
+// also summed, as unevaluated f32 pairs (as the reference sums them in
 // double-float, lennard_jones.wgsl:518-519). Every thread of the block must
-// call this (it synchronises the block and ends in shuffles); on return the
-// four lanes of a particle hold its totals.
+// call this: it synchronises the block between tiles.
 template <bool SHIFTED_FORCE, bool ENERGIES>
 __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap* map,
                                                     const Arena& a, const Box& bx, uint32_t i,
-                                                    uint32_t sub, bool valid,
-                                                    const uint4* __restrict__ cur) {
+                                                    bool valid, const uint4* __restrict__ cur) {
     PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u};
-    const uint32_t first = blockIdx.x * kBlockParticles;
-    const uint32_t p = threadIdx.x / kLanes;
+    const uint32_t first = blockIdx.x * kForceThreads;
     const uint32_t rows = (a.glob->max_count + 3u) / 4u;
-    const uint32_t tiles = (rows + kStageRows - 1u) / kStageRows;
+    const uint32_t tiles = (rows + kTileRows - 1u) / kTileRows;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < kStageSlots; k++) bar_init(&st.bar[k]);
+        for (int k = 0; k < kTileSlots; k++) bar_init(&st.bar[k]);
         init_fence();
     }
     __syncthreads();
     if (threadIdx.x == 0)
-        for (uint32_t t = 0; t < tiles && t < (uint32_t)kStageSlots; t++)
-            tile_load(map, &st.rows[t][0][0], &st.bar[t], (int)(first * 4u), (int)(t * kStageRows));
+        for (uint32_t t = 0; t < tiles && t < (uint32_t)kTileSlots; t++)
+            tile_load(map, &st.rows[t][0][0], &st.bar[t], (int)(first * 2u), (int)(t * kTileRows));
 
     uint4 own = make_uint4(0u, 0u, 0u, 0u);
     uint32_t cnt = 0;
@@ -120,16 +116,17 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         own = __ldg(cur + i);
         cnt = __ldg(a.list_count + i);
     }
+    const uint32_t my_rows = (cnt + 3u) / 4u;
     const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
     const float fshift = bx.force_shift;
-    auto accumulate = [&](const uint4 pj) {
+    auto accumulate = [&](const uint4 pj, bool live) {
         const float dx = decode_diff(pj.x, own.x, dec0);
         const float dy = decode_diff(pj.y, own.y, dec1);
         const float dz = decode_diff(pj.z, own.z, dec2);
         const float r2 = dx * dx + dy * dy + dz * dz;
-        const bool in = r2 < rc2;
-        // branch-free: most list entries are inside the cutoff and the pair
-        // math is finite for all of them
+        const bool in = live && r2 < rc2;
+        // branch-free: most list entries are inside the cutoff; the select
+        // drops whatever the pair math gives for entries that are not
         const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
         s.ax -= dx * f;
         s.ay -= dy * f;
@@ -149,38 +146,35 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
 
     bool lost = false;
     for (uint32_t t = 0; t < tiles; t++) {
-        const uint32_t slot = t % kStageSlots;
-        const bool ok = bar_wait(&st.bar[slot], (t / kStageSlots) & 1u);
+        const uint32_t slot = t % kTileSlots;
+        const bool ok = bar_wait(&st.bar[slot], (t / kTileSlots) & 1u);
         if (__syncthreads_or(!ok)) {
             lost = true;
             break;
         }
-        const uint32_t* tile = reinterpret_cast<const uint32_t*>(&st.rows[slot][0][0]);
-        const uint32_t k0 = t * kStageRows * 4u + sub;  // this lane's first entry in the tile
-        // four entries per round: indices from shared memory, then all four
-        // gathers, then the arithmetic
 #pragma unroll
-        for (int half = 0; half < kStageRows; half += 4) {
-            uint32_t j[4];
-            bool use[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const uint32_t k = k0 + (uint32_t)(half + r) * 4u;
-                use[r] = k < cnt;
-                j[r] = use[r] ? tile[((half + r) * kBlockParticles + p) * 4u + sub] : i;
+        for (int r = 0; r < kTileRows; r++) {
+            const uint32_t row = t * kTileRows + (uint32_t)r;
+            if (row < my_rows) {
+                // one row: four entries, the last ones live only up to cnt
+                const uint4 e = st.rows[slot][r][threadIdx.x];
+                const uint32_t k = row * 4u;
+                const bool l1 = k + 1u < cnt, l2 = k + 2u < cnt, l3 = k + 3u < cnt;
+                const uint4 p0 = __ldg(cur + e.x);
+                const uint4 p1 = l1 ? __ldg(cur + e.y) : own;
+                const uint4 p2 = l2 ? __ldg(cur + e.z) : own;
+                const uint4 p3 = l3 ? __ldg(cur + e.w) : own;
+                accumulate(p0, true);
+                accumulate(p1, l1);
+                accumulate(p2, l2);
+                accumulate(p3, l3);
             }
-            uint4 pj[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) pj[r] = use[r] ? __ldg(cur + j[r]) : own;
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-                if (use[r]) accumulate(pj[r]);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && t + kStageSlots < tiles) {
+        if (threadIdx.x == 0 && t + kTileSlots < tiles) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tile_load(map, &st.rows[slot][0][0], &st.bar[slot], (int)(first * 4u),
-                      (int)((t + kStageSlots) * kStageRows));
+            tile_load(map, &st.rows[slot][0][0], &st.bar[slot], (int)(first * 2u),
+                      (int)((t + kTileSlots) * kTileRows));
         }
     }
     if (lost) {
@@ -188,65 +182,51 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         // the block's shared memory goes away
         if (threadIdx.x == 0) {
             atomicCAS(&a.glob->fault, 0u, kFaultTmaTimeout);
-            for (uint32_t t = 0; t < tiles && t < (uint32_t)kStageSlots; t++)
+            for (uint32_t t = 0; t < tiles && t < (uint32_t)kTileSlots; t++)
                 bar_wait(&st.bar[t], 0u);
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int o = 1; o < kLanes; o <<= 1) {
-        s.ax += __shfl_xor_sync(kFull, s.ax, o);
-        s.ay += __shfl_xor_sync(kFull, s.ay, o);
-        s.az += __shfl_xor_sync(kFull, s.az, o);
-        if (ENERGIES) {
-            float t, e;
-            const float pe = __shfl_xor_sync(kFull, s.pe, o), pl = __shfl_xor_sync(kFull, s.pe_lo, o);
-            two_sum(s.pe, pe, t, e);
-            s.pe = t;
-            s.pe_lo = (s.pe_lo + pl) + e;
-            const float w = __shfl_xor_sync(kFull, s.w, o), wl = __shfl_xor_sync(kFull, s.w_lo, o);
-            two_sum(s.w, w, t, e);
-            s.w = t;
-            s.w_lo = (s.w_lo + wl) + e;
-            s.near += __shfl_xor_sync(kFull, s.near, o);
-        }
-    }
     return s;
 }
 
-__device__ __forceinline__ float component(const PairSums& s, uint32_t k) {
-    return k == 0 ? s.ax : (k == 1 ? s.ay : s.az);
-}
-
-// Langevin noise for coordinate k of a particle: Philox-4x32-10 (Salmon et
-// al., SC'11) with counter (id, step lo, step hi, 0) and key (seed, "LJV1");
+// Langevin noise of a particle at a step: Philox-4x32-10 (Salmon et al.,
+// SC'11) with counter (id, step lo, step hi, 0) and key (seed, "LJV1");
 // uniforms in (0, 1] from 24 bits as the reference's uniform01
 // (lennard_jones.wgsl:175-178); Box-Muller in f32: x and y from the first
 // pair of uniforms (cosine and sine), z from the second (cosine).
-__device__ __forceinline__ float langevin_component(uint32_t id, unsigned long long step,
-                                                   uint32_t seed, uint32_t k) {
+__device__ __forceinline__ void langevin_noise(uint32_t id, unsigned long long step,
+                                               uint32_t seed, float xi[3]) {
     const uint4 r = philox(id, step, seed);
-    const uint32_t ra = k < 2 ? r.x : r.z, rb = k < 2 ? r.y : r.w;
-    const float ua = __fdiv_rn((float)(ra >> 8) + 1.0f, 16777216.0f);
-    const float ub = __fdiv_rn((float)(rb >> 8) + 1.0f, 16777216.0f);
-    const float radius = sqrtf(-2.0f * logf(ua));
-    const float angle = 6.283185307179586f * ub;
-    return k == 1 ? radius * sinf(angle) : radius * cosf(angle);
+    const float u0 = __fdiv_rn((float)(r.x >> 8) + 1.0f, 16777216.0f);
+    const float u1 = __fdiv_rn((float)(r.y >> 8) + 1.0f, 16777216.0f);
+    const float u2 = __fdiv_rn((float)(r.z >> 8) + 1.0f, 16777216.0f);
+    const float u3 = __fdiv_rn((float)(r.w >> 8) + 1.0f, 16777216.0f);
+    const float ra = sqrtf(-2.0f * logf(u0));
+    const float aa = 6.283185307179586f * u1;
+    const float rb = sqrtf(-2.0f * logf(u2));
+    const float ab = 6.283185307179586f * u3;
+    xi[0] = ra * cosf(aa);
+    xi[1] = ra * sinf(aa);
+    xi[2] = rb * cosf(ab);
 }
 
 // ---- prime (lennard_jones.wgsl:547-553): first forces; the stored velocity
 // becomes half a kick behind the given one ----
 template <bool SHIFTED_FORCE>
-__global__ void __launch_bounds__(kBlock) prime_kernel(Arena a, const __grid_constant__ CUtensorMap map) {
+__global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
+                                                              const __grid_constant__ CUtensorMap map) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
     const bool valid = i < a.nslots;
     const Box& bx = a.boxes[valid ? box_of_slot(a, i) : 0u];
-    const PairSums s = block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, sub, valid,
-                                                             a.cache[a.glob->phase]);
-    if (valid && sub < 3) a.v[sub * a.seg + i] -= (double)component(s, sub) * bx.half_dt;
+    const PairSums s =
+        block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, valid, a.cache[a.glob->phase]);
+    if (!valid) return;
+    a.v[i] -= (double)s.ax * bx.half_dt;
+    a.v[a.seg + i] -= (double)s.ay * bx.half_dt;
+    a.v[2 * (size_t)a.seg + i] -= (double)s.az * bx.half_dt;
 }
 
 // ---- one step: begin + force_kick of the reference fused
@@ -259,45 +239,48 @@ __global__ void __launch_bounds__(kBlock) prime_kernel(Arena a, const __grid_con
 // step's), and the largest squared displacement since the last list build
 // feeds the next step's rebuild decision.
 template <bool SHIFTED_FORCE>
-__global__ void __launch_bounds__(kBlock) step_kernel(Arena a, const __grid_constant__ CUtensorMap map) {
+__global__ void __launch_bounds__(kForceThreads) step_kernel(Arena a,
+                                                             const __grid_constant__ CUtensorMap map) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
     const bool valid = i < a.nslots;
     const uint32_t phase = a.glob->phase;
     const uint32_t b = valid ? box_of_slot(a, i) : 0u;
     const Box& bx = a.boxes[b];
-    const PairSums s =
-        block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, sub, valid, a.cache[phase]);
-    uint32_t enc = 0;
-    float d2 = 0.0f;
-    if (valid && sub < 3) {
-        const size_t q = (size_t)sub * a.seg + i;
-        double x = a.x[q];
-        double v = a.v[q] + (double)component(s, sub) * bx.dt;
-        if (bx.thermostat == 1) {
-            const float xi = langevin_component(a.id[i], a.glob->step, bx.seed, sub);
-            x += v * bx.half_dt;
-            v = bx.c1 * v + bx.c2 * (double)xi;
-            x += v * bx.half_dt;
-        } else {
-            x += v * bx.dt;
+    const PairSums s = block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, valid, a.cache[phase]);
+    float disp2 = 0.0f;
+    if (valid) {
+        const float acc[3] = {s.ax, s.ay, s.az};
+        float xi[3] = {0.0f, 0.0f, 0.0f};
+        const bool langevin = bx.thermostat == 1;
+        if (langevin) langevin_noise(a.id[i], a.glob->step, bx.seed, xi);
+        const uint4 snap = a.snap[i];
+        const uint32_t sw[3] = {snap.x, snap.y, snap.z};
+        uint32_t enc[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t q = (size_t)k * a.seg + i;
+            double x = a.x[q];
+            double v = a.v[q] + (double)acc[k] * bx.dt;
+            if (langevin) {
+                x += v * bx.half_dt;
+                v = bx.c1 * v + bx.c2 * (double)xi[k];
+                x += v * bx.half_dt;
+            } else {
+                x += v * bx.dt;
+            }
+            x = wrap(x, bx.box[k]);
+            a.x[q] = x;
+            a.v[q] = v;
+            enc[k] = encode(x, bx.enc[k]);
+            const float d = decode_diff(enc[k], sw[k], bx.dec[k]);
+            disp2 += d * d;
         }
-        x = wrap(x, bx.box[sub]);
-        a.x[q] = x;
-        a.v[q] = v;
-        enc = encode(x, bx.enc[sub]);
-        const uint32_t snap = reinterpret_cast<const uint32_t*>(a.snap + i)[sub];
-        const float d = decode_diff(enc, snap, bx.dec[sub]);
-        d2 = d * d;
+        a.cache[phase ^ 1u][i] = make_uint4(enc[0], enc[1], enc[2], 0u);
     }
-    const uint32_t e1 = __shfl_down_sync(kFull, enc, 1), e2 = __shfl_down_sync(kFull, enc, 2);
-    const float d21 = __shfl_down_sync(kFull, d2, 1), d22 = __shfl_down_sync(kFull, d2, 2);
-    const bool lead = valid && sub == 0;
-    if (lead) a.cache[phase ^ 1u][i] = make_uint4(enc, e1, e2, 0u);
-    block_max_per_box(a, lead, b, blockIdx.x * kBlockParticles, d2 + d21 + d22);
-    if (tid == 0) a.glob->pending = 1u;
+    block_max_per_box(a, valid, b, blockIdx.x * kForceThreads, disp2);
+    if (i == 0) a.glob->pending = 1u;
 }
 
 // ---- measure (lennard_jones.wgsl:576-626) ----
@@ -306,47 +289,42 @@ __global__ void __launch_bounds__(kBlock) step_kernel(Arena a, const __grid_cons
 // kick), kinetic energy and momentum in f64. Each value goes to 32.32 fixed
 // point scaled like the reference and is summed exactly.
 template <bool SHIFTED_FORCE>
-__global__ void __launch_bounds__(kBlock) measure_kernel(Arena a, const __grid_constant__ CUtensorMap map,
-                                                         int canonical) {
+__global__ void __launch_bounds__(kForceThreads) measure_kernel(Arena a,
+                                                                const __grid_constant__ CUtensorMap map,
+                                                                int canonical) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t i = tid / kLanes, sub = tid % kLanes;
+    const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
     const bool valid = i < a.nslots;
     const uint32_t b = valid ? box_of_slot(a, i) : 0u;
     const Box& bx = a.boxes[b];
-    const PairSums s = block_pair_sums<SHIFTED_FORCE, true>(st, &map, a, bx, i, sub, valid,
-                                                            a.cache[a.glob->phase]);
-    double vel = 0.0;
-    if (valid && sub < 3) {
-        vel = a.v[(size_t)sub * a.seg + i] + (double)component(s, sub) * bx.half_dt;
-        if (canonical) a.vcanon[(size_t)sub * a.seg + i] = vel;
-    }
-    const double vy = __shfl_down_sync(kFull, vel, 1), vz = __shfl_down_sync(kFull, vel, 2);
-    const bool lead = valid && sub == 0;
+    const PairSums s =
+        block_pair_sums<SHIFTED_FORCE, true>(st, &map, a, bx, i, valid, a.cache[a.glob->phase]);
     long long v[kSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (lead) {
-        const double vx = vel;
-        double ke = 0.0;
-        ke += vx * vx;
-        ke += vy * vy;
-        ke += vz * vz;
+    if (valid) {
+        const float acc[3] = {s.ax, s.ay, s.az};
+        double vel[3], ke = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            vel[k] = a.v[(size_t)k * a.seg + i] + (double)acc[k] * bx.half_dt;
+            ke += vel[k] * vel[k];
+            if (canonical) a.vcanon[(size_t)k * a.seg + i] = vel[k];
+        }
         ke *= 0.5;
         const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
         v[0] = fixed_raw_f64(ke * es);
         v[1] = fixed_raw_f32(s.pe * bx.energy_scale) + fixed_raw_f32(s.pe_lo * bx.energy_scale);
         v[2] = fixed_raw_f32(s.w * bx.energy_scale) + fixed_raw_f32(s.w_lo * bx.energy_scale);
-        v[3] = fixed_raw_f64(vx * ms);
-        v[4] = fixed_raw_f64(vy * ms);
-        v[5] = fixed_raw_f64(vz * ms);
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[3 + k] = fixed_raw_f64(vel[k] * ms);
         v[6] = s.near >= bx.near_count ? (1ll << 32) : 0ll;
         a.pe_half[2 * i] = s.pe;
         a.pe_half[2 * i + 1] = s.pe_lo;
         a.w_half[2 * i] = s.w;
         a.w_half[2 * i + 1] = s.w_lo;
-        a.vel4[i] = make_float4((float)vx, (float)vy, (float)vz, (float)s.near);
+        a.vel4[i] = make_float4((float)vel[0], (float)vel[1], (float)vel[2], (float)s.near);
     }
-    block_sum_slots(a, lead, b, blockIdx.x * kBlockParticles, v);
+    block_sum_slots(a, valid, b, blockIdx.x * kForceThreads, v);
 }
 
 // ---- FP32 calibration: eight independent FMA chains per thread, so the
@@ -368,33 +346,33 @@ __global__ void __launch_bounds__(kBlock) fp32_peak_kernel(float* out, int iters
 
 // ---- launchers ----
 static unsigned particle_blocks(const Arena& a) {
-    return blocks_for((uint64_t)a.nslots * kLanes);
+    return blocks_for(a.nslots, kForceThreads);
 }
 
 cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_force,
                          cudaStream_t s) {
     if (shifted_force)
-        prime_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+        prime_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     else
-        prime_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+        prime_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     return after_launch();
 }
 
 cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
                         cudaStream_t s) {
     if (shifted_force)
-        step_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+        step_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     else
-        step_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map);
+        step_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     return after_launch();
 }
 
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_force,
                            bool canonical, cudaStream_t s) {
     if (shifted_force)
-        measure_kernel<true><<<particle_blocks(a), kBlock, 0, s>>>(a, map, canonical ? 1 : 0);
+        measure_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, canonical ? 1 : 0);
     else
-        measure_kernel<false><<<particle_blocks(a), kBlock, 0, s>>>(a, map, canonical ? 1 : 0);
+        measure_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, canonical ? 1 : 0);
     return after_launch();
 }
 

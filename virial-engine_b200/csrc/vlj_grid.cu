@@ -294,144 +294,6 @@ __global__ void pack_kernel(Arena a) {
     a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
 }
 
-// ---- Verlet list build (lennard_jones.wgsl:454-499) ----
-// Everything within cutoff + skin, cells in the order dz, dy, dx = -1..1 with
-// periodic wrap, then each cell in sorted order; one thread per particle.
-// Acceptance is the reference's f32 test on packed positions, operation for
-// operation, so the list is the reference's entry for entry. Two cheaper,
-// exact shortcuts keep that order:
-//  - a neighbour cell whose box lies farther from the particle than the list
-//    radius (plus a margin) cannot hold a list entry and is skipped;
-//  - a test on the 32-bit encoded positions settles every candidate farther
-//    than sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in): the
-//    two radii bracket list_r2 by more than the reference's f32 separations
-//    and the encoded ones can differ, so only candidates in the thin shell
-//    between them need the reference's own arithmetic.
-struct RefTest {
-    float xh[3], xl[3], side[3], inv[3], list_r2;
-    const float* q510;
-    // the reference's predicate for a packed neighbour position
-    __device__ __forceinline__ bool operator()(const float4 pj) const {
-        const uint32_t bits = __float_as_uint(pj.w);
-        const float ph[3] = {pj.x, pj.y, pj.z};
-        float d[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const float lo = __fmul_rn(q510[(bits >> (9u * k)) & 511u], last_bit(ph[k]));
-            const float e = __fadd_rn(__fsub_rn(ph[k], xh[k]), __fsub_rn(lo, xl[k]));
-            d[k] = nearest_ref_fast(e, side[k], inv[k]);
-        }
-        const float r2 =
-            __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2]));
-        return r2 < list_r2;
-    }
-};
-
-__global__ void __launch_bounds__(kBlock) build_list_kernel(Arena a) {
-    count_kernel(a);
-    if (!a.glob->any) return;
-    __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
-    for (int t = threadIdx.x; t < 512; t += blockDim.x)
-        s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
-    __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
-    const uint32_t b = box_of_slot(a, i);
-    if (!rebuilding(a, b)) return;
-    const Box& bx = a.boxes[b];
-    const uint4* __restrict__ cur = a.cache[a.glob->phase];
-    const uint4 own_enc = cur[i];
-    const float4 own = a.ref[i];
-    const float4 own_lo = a.ref_lo[i];
-    RefTest test;
-    test.xh[0] = own.x, test.xh[1] = own.y, test.xh[2] = own.z;
-    test.xl[0] = own_lo.x, test.xl[1] = own_lo.y, test.xl[2] = own_lo.z;
-    for (int k = 0; k < 3; k++) {
-        test.side[k] = bx.box_f[k];
-        test.inv[k] = bx.inv_box_f[k];
-    }
-    test.list_r2 = bx.list_r2;
-    test.q510 = s_q510;
-    const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
-    const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};
-    const int32_t ci = (int32_t)(a.cell_of_slot[i] - bx.cell_base);
-    const int32_t c[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
-    // squared distance from the particle to the faces of its cell, per axis
-    // and side, less a margin for the f32 binning: a neighbour cell farther
-    // than the list radius by these bounds holds no list entry
-    float gap2[3][2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const float lo = (float)c[k] * bx.cell_size_f[k];
-        const float below = fmaxf(test.xh[k] - lo - 1e-3f, 0.0f);
-        const float above = fmaxf(lo + bx.cell_size_f[k] - test.xh[k] - 1e-3f, 0.0f);
-        gap2[k][0] = below * below;
-        gap2[k][1] = above * above;
-    }
-    const uint32_t cap = bx.capacity;
-    const float pre_r2 = bx.prefilter_r2, acc_r2 = bx.accept_r2;
-    uint32_t found = 0;
-    auto take = [&](uint32_t j, uint4 pe) {
-        const float r2e = encoded_r2(pe, own_enc, dec);
-        bool in;
-        if (r2e < acc_r2)
-            in = true;
-        else if (r2e < pre_r2)
-            in = test(a.ref[j]);
-        else
-            return;
-        if (in) {
-            if (found < cap) a.list[((size_t)(found >> 2) * a.seg + i) * 4u + (found & 3u)] = j;
-            found += 1;
-        }
-    };
-    for (int32_t dz = -1; dz <= 1; dz++) {
-        const float gz = dz == 0 ? 0.0f : gap2[2][dz > 0];
-        if (gz > pre_r2) continue;
-        int32_t uz = c[2] + dz;
-        uz = uz < 0 ? uz + n[2] : (uz >= n[2] ? uz - n[2] : uz);
-        for (int32_t dy = -1; dy <= 1; dy++) {
-            const float gzy = gz + (dy == 0 ? 0.0f : gap2[1][dy > 0]);
-            if (gzy > pre_r2) continue;
-            int32_t uy = c[1] + dy;
-            uy = uy < 0 ? uy + n[1] : (uy >= n[1] ? uy - n[1] : uy);
-            const uint32_t row = bx.cell_base + ((uint32_t)uz * (uint32_t)n[1] + (uint32_t)uy) * (uint32_t)n[0];
-            for (int32_t dx = -1; dx <= 1; dx++) {
-                if (gzy + (dx == 0 ? 0.0f : gap2[0][dx > 0]) > pre_r2) continue;
-                int32_t ux = c[0] + dx;
-                ux = ux < 0 ? ux + n[0] : (ux >= n[0] ? ux - n[0] : ux);
-                const uint32_t cell = row + (uint32_t)ux;
-                const uint32_t end = a.cell_start[cell + 1];
-                uint32_t t = a.cell_start[cell];
-                // two candidates per round, both gathers in flight together
-                for (; t + 1 < end; t += 2) {
-                    const uint32_t j0 = a.sorted[t], j1 = a.sorted[t + 1];
-                    const uint4 p0 = __ldg(cur + j0), p1 = __ldg(cur + j1);
-                    if (j0 != i) take(j0, p0);
-                    if (j1 != i) take(j1, p1);
-                }
-                if (t < end) {
-                    const uint32_t j0 = a.sorted[t];
-                    if (j0 != i) take(j0, __ldg(cur + j0));
-                }
-            }
-        }
-    }
-    const uint32_t kept = found < cap ? found : cap;
-    a.list_count[i] = kept;
-    if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
-    a.snap[i] = own_enc;
-    // the longest list, one atomic per warp when the whole warp is here
-    if (__activemask() == 0xffffffffu) {
-        uint32_t m = kept;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31u) == 0) atomicMax(&a.glob->max_count, m);
-    } else {
-        atomicMax(&a.glob->max_count, kept);
-    }
-}
-
 // ---- launchers ----
 cudaError_t launch_encode(const Arena& a, cudaStream_t s) {
     encode_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
@@ -454,7 +316,7 @@ cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
     sort_kernel<<<blocks_for((uint64_t)a.ncells * 32u), kBlock, 0, s>>>(a);
     reorder_kernel<<<slots, kBlock, 0, s>>>(a);
     pack_kernel<<<slots, kBlock, 0, s>>>(a);
-    build_list_kernel<<<slots, kBlock, 0, s>>>(a);
+    launch_build_list(a, s);  // vlj_build.cu
     return after_launch(7);
 }
 

@@ -37,10 +37,20 @@ namespace vlj {
 
 constexpr int kBlock = 256;
 constexpr int kSlots = 8;  // measurement accumulators per box
-constexpr int kLanes = 4;  // threads per particle in the force kernels
-constexpr int kBlockParticles = kBlock / kLanes;
-constexpr int kStageRows = 8;   // list rows (32 entries per particle) per TMA tile
-constexpr int kStageSlots = 3;  // tiles in flight per block
+// Force kernels: one thread per particle, kForceThreads per block; each TMA
+// tile holds kTileRows list rows (4 entries each) of the block's particles.
+// The tile ring's shared memory comes out of the same 256 KB per SM as the L1
+// that serves the neighbour gathers, so its depth is a tuning knob
+// (build.py --tune sweeps it).
+#ifndef VLJ_TILE_ROWS
+#define VLJ_TILE_ROWS 4
+#endif
+#ifndef VLJ_TILE_SLOTS
+#define VLJ_TILE_SLOTS 3
+#endif
+constexpr int kForceThreads = 128;
+constexpr int kTileRows = VLJ_TILE_ROWS;
+constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block
 // measurement slots: 0 kinetic, 1 potential, 2 virial, 3-5 momentum,
 // 6 condensed count, 7 unused (lennard_jones.wgsl:576-626)
 
@@ -61,6 +71,7 @@ struct Box {
     float inv_box_f[3];  // 1 / box_f, for nearest_ref_fast
     float prefilter_r2;  // list_r2 widened past any encoding difference
     float accept_r2;     // list_r2 narrowed past any encoding difference
+    float reach_r2;      // prefilter_r2 widened past binning round-off
     uint32_t cells[3];
     uint32_t total_cells;
     uint32_t cell_base;  // first cell of this box
@@ -279,8 +290,9 @@ cudaError_t launch_encode(const Arena& a, cudaStream_t s);
 cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle);
 cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
 // The force kernels read list rows through `list_map`: a 2D TMA tensor map
-// over the list (inner dimension 4 * seg u32, outer one row per four
-// entries) whose box is kStageRows rows of kBlockParticles slots.
+// over the list viewed as u64 pairs of entries (inner dimension 2 * seg,
+// outer one row per four entries) whose box is kTileRows rows of
+// kForceThreads slots.
 cudaError_t launch_prime(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                          cudaStream_t s);
 cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifted_force,

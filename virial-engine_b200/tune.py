@@ -1,0 +1,79 @@
+"""Autotuner for the force kernels' TMA tile ring.
+
+The list rows staged in shared memory and the L1 that serves the neighbour
+gathers share each SM's 256 KB, so the tile depth (rows per tile, tiles in
+flight) trades list-stream latency against gather hit rate. This builds one
+library per candidate into build/tune/ (git-ignored), times the step kernel on
+a workload in a child process per variant (CUDA events around every launch,
+L2 flushed between steps), and prints the ranking as JSON lines. Needs a GPU.
+
+    python virial-engine_b200/tune.py [--cells 40] [--steps 60]
+
+The winner becomes the default of VLJ_TILE_ROWS / VLJ_TILE_SLOTS in
+csrc/vlj_internal.cuh.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT_DIR = os.path.join(HERE, "build", "tune")
+CANDIDATES = [(1, 4), (1, 6), (2, 3), (2, 4), (4, 2), (4, 3), (8, 2)]
+
+
+def child(lib, cells, steps):
+    os.environ["VLJ_LIBRARY"] = lib
+    sys.path.insert(0, HERE)
+    import torch
+    import virial_lj as vl
+    p, box = vl.lattice_fcc(cells, 0.8442, 1.0, 7)
+    stream = torch.cuda.Stream()
+    sim = vl.LennardJones(p, vl.Settings([box] * 3, dt=0.005, shifted_force=True,
+                                         thermostat=vl.Langevin(1.0, 1.0, 7)),
+                          stream=stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sim.step(10)
+    sim.kernel_timing(True)
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        sim.step(1)
+    ms, n = sim.kernel_time()
+    print(json.dumps({"step_kernel_us": ms * 1e3 / n, "launches": n}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cells", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--child", default=None)
+    args = ap.parse_args()
+    if args.child:
+        child(args.child, args.cells, args.steps)
+        return
+    sys.path.insert(0, HERE)
+    import build
+    os.makedirs(OUT_DIR, exist_ok=True)
+    results = []
+    for rows, slots in CANDIDATES:
+        lib = os.path.join(OUT_DIR, f"libvirial_lj_r{rows}_s{slots}.so")
+        build.build(defines={"VLJ_TILE_ROWS": rows, "VLJ_TILE_SLOTS": slots}, out=lib)
+        out = subprocess.run([sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
+                              "--steps", str(args.steps)], capture_output=True, text=True)
+        if out.returncode != 0:
+            print(json.dumps({"rows": rows, "slots": slots, "error": out.stderr[-500:]}), flush=True)
+            continue
+        r = json.loads(out.stdout.strip().splitlines()[-1])
+        r.update(rows=rows, slots=slots)
+        results.append(r)
+        print(json.dumps(r), flush=True)
+    if results:
+        best = min(results, key=lambda r: r["step_kernel_us"])
+        print(json.dumps({"best": best}))
+
+
+if __name__ == "__main__":
+    main()

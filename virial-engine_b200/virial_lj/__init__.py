@@ -46,7 +46,7 @@ def _check(status):
 
 
 def library_path():
-    return _ffi.LIB_PATH
+    return _lib._name
 
 
 def device_count():

@@ -116,8 +116,10 @@ SIGNATURES = {
 }
 
 
-def load(path=LIB_PATH):
-    """Load the CUDA library; raises if it has not been built."""
+def load(path=None):
+    """Load the CUDA library (VLJ_LIBRARY overrides the in-tree build, e.g.
+    for a tuning variant); raises if it has not been built."""
+    path = path or os.environ.get("VLJ_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(
             f"{path} is missing: build the CUDA library first (python virial-engine_b200/build.py)")
