@@ -239,6 +239,33 @@ VLJ_API vlj_status vlj_batch_measure(vlj_batch *batch, vlj_measurement *out);
 VLJ_API vlj_status vlj_batch_read_particles(vlj_batch *batch, size_t replica, vlj_particle *out);
 VLJ_API vlj_status vlj_batch_count(const vlj_batch *batch, size_t *replicas, uint64_t *particles);
 
+/* ---- cell binning that allocates no device memory ----
+ * No counterpart in the reference. For callers that cannot let a library
+ * allocate: an embedding framework that hands out all device memory from its
+ * own pool, or a latency-critical loop where cudaMalloc / cudaFree would
+ * synchronise the device and stall other streams. The caller passes every
+ * buffer; this call allocates nothing.
+ *
+ * Bins `count` positions (device memory, count x 3 doubles, row-major, each
+ * inside [0, box_size)) into cells[0] x cells[1] x cells[2] cells the way the
+ * simulation bins them (the reference's grid.wgsl: clamp(floor(f32(x) /
+ * cell size)), cell index (z * ny + y) * nx + x, a stable counting sort).
+ * Outputs, all device memory the caller owns: sorted[count] (particle indices
+ * in cell order, index order within a cell), cell_start[cells + 1],
+ * cell_of[count]. Work is enqueued on `stream` (a cudaStream_t, or NULL).
+ *
+ * Limits and sharing: at most VLJ_BIN_NOALLOC_MAX_CELLS cells (larger grids
+ * are rejected with VLJ_INVALID_ARG). The per-cell counters live in one fixed
+ * device array (VLJ_BIN_NOALLOC_MAX_CELLS x 4 bytes) that every GPU loading
+ * the library holds until exit and that every call shares: calls whose work
+ * overlaps on the GPU race with each other, so serialise them (one stream, or
+ * events). The first call on a device looks up that array's address and
+ * should come before any stream capture. */
+#define VLJ_BIN_NOALLOC_MAX_CELLS 262144u
+VLJ_API vlj_status vlj_bin_noalloc(const double *pos, size_t count, const double box_size[3],
+                                   const uint32_t cells[3], uint32_t *sorted,
+                                   uint32_t *cell_start, uint32_t *cell_of, void *stream);
+
 /* ---- inspection for tests (no reference counterpart) ----
  * Reads the grid and lists of the last rebuild: slot of each position in
  * cell order (`sorted`, n), cell starts (total_cells + 1), cell of each slot
