@@ -273,6 +273,7 @@ vlj_sim::~vlj_sim() {
     if (pin_x) cudaFreeHost(pin_x);
     if (pin_v) cudaFreeHost(pin_v);
     if (pin_id) cudaFreeHost(pin_id);
+    if (series) cudaFree(series);
     for (int k = 0; k < kRing; k++)
         if (ring_event[k]) cudaEventDestroy(ring_event[k]);
     if (ring) cudaFreeHost(ring);
@@ -730,6 +731,8 @@ vlj_status check_fault(vlj_sim* s) {
     return VLJ_OK;
 }
 
+vlj_status sim_lists_now(vlj_sim* s) { return lists_now(s); }
+
 vlj_status sim_allocate(vlj_sim* s, void* stream) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
@@ -780,6 +783,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.w_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.vel4, seg));
     TRY(dalloc(s, &a.vcanon, 3 * (size_t)seg));
+    if (s->box.profile_bins)
+        TRY(dalloc(s, &a.profile, (size_t)s->box.profile_bins * 8 + 3));
     // the last cell of the box ends at the last slot
     CUDA_TRY(cudaMemcpy(a.cell_start + a.ncells, &n, sizeof n, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(d_box, &s->box, sizeof(Box), cudaMemcpyHostToDevice));

@@ -299,8 +299,11 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifte
                         cudaStream_t s);
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                            bool canonical, cudaStream_t s);
-cudaError_t launch_profile(const Arena& a, bool shifted_force, cudaStream_t s);
-cudaError_t launch_heat_current(const Arena& a, bool shifted_force, cudaStream_t s);
+// Sampling kernels (vlj_sampling.cu): one profile sample added into
+// a.profile, one heat-current sample into a.series slot 1 + 3 * sample.
+cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cudaStream_t s);
+cudaError_t launch_heat_current(const Arena& a, bool shifted_force, uint32_t sample,
+                                cudaStream_t s);
 cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s);
 unsigned long long launches();
 

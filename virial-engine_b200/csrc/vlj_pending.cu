@@ -5,12 +5,6 @@
 using vlj::fail;
 
 extern "C" {
-vlj_status vlj_sample_profile(vlj_sim*) { return fail(VLJ_NOT_ENABLED, "profiles are not available yet"); }
-vlj_status vlj_clear_profile(vlj_sim*) { return fail(VLJ_NOT_ENABLED, "profiles are not available yet"); }
-vlj_status vlj_read_profile(vlj_sim*, vlj_slab*, double*, uint64_t*) { return fail(VLJ_NOT_ENABLED, "profiles are not available yet"); }
-vlj_status vlj_record_heat_current(vlj_sim*, uint32_t) { return fail(VLJ_NOT_ENABLED, "heat current is not available yet"); }
-vlj_status vlj_sample_heat_current(vlj_sim*) { return fail(VLJ_NOT_ENABLED, "heat current is not available yet"); }
-vlj_status vlj_read_heat_current(vlj_sim*, double*, size_t, size_t*) { return fail(VLJ_NOT_ENABLED, "heat current is not available yet"); }
 vlj_status vlj_batch_create(const vlj_replica_desc*, size_t, double, double, double, int32_t, void*, vlj_batch**) { return fail(VLJ_NOT_ENABLED, "batches are not available yet"); }
 vlj_status vlj_batch_destroy(vlj_batch*) { return VLJ_OK; }
 vlj_status vlj_batch_step(vlj_batch*, uint32_t) { return fail(VLJ_NOT_ENABLED, "batches are not available yet"); }

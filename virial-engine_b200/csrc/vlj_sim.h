@@ -50,6 +50,8 @@ struct vlj_sim {
     uint64_t profile_samples = 0;
     // heat current series
     uint32_t series_samples = 0;
+    uint32_t series_capacity = 0;
+    unsigned long long* series = nullptr;  // owned here (reallocated by record)
     // pinned staging for particle uploads and read-backs (x, v: 3 * seg; id: seg)
     double* pin_x = nullptr;
     double* pin_v = nullptr;
@@ -71,6 +73,8 @@ struct vlj_sim {
 namespace vlj {
 vlj_status sim_allocate(vlj_sim* s, void* stream);
 vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out);
+// Decide and, when due, rebuild the lists now (positions are about to be read).
+vlj_status sim_lists_now(vlj_sim* s);
 vlj_status check_fault(vlj_sim* s);
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
 }  // namespace vlj
