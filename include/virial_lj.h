@@ -233,11 +233,15 @@ VLJ_API vlj_status vlj_batch_create(const vlj_replica_desc *replicas, size_t cou
                                     void *stream, vlj_batch **out);
 VLJ_API vlj_status vlj_batch_destroy(vlj_batch *batch);
 VLJ_API vlj_status vlj_batch_step(vlj_batch *batch, uint32_t steps);
+/* Step, then wait for the steps to finish. */
+VLJ_API vlj_status vlj_batch_run(vlj_batch *batch, uint64_t steps);
 /* One measurement per replica into out[replicas]; waits. */
 VLJ_API vlj_status vlj_batch_measure(vlj_batch *batch, vlj_measurement *out);
 /* Replica r's particles into out (its count), input order; waits. */
 VLJ_API vlj_status vlj_batch_read_particles(vlj_batch *batch, size_t replica, vlj_particle *out);
 VLJ_API vlj_status vlj_batch_count(const vlj_batch *batch, size_t *replicas, uint64_t *particles);
+/* Replica r's box sides as the simulation uses them (rounded to f32). */
+VLJ_API vlj_status vlj_batch_box_size(const vlj_batch *batch, size_t replica, double out[3]);
 
 /* ---- cell binning that allocates no device memory ----
  * No counterpart in the reference. For callers that cannot let a library
@@ -310,6 +314,10 @@ VLJ_API vlj_status vlj_debug_kernel_time(vlj_sim *sim, double *total_ms, uint64_
 /* FP32 FMA throughput of the current device in TFLOP/s (a calibration kernel
  * of independent FMA chains on every SM). */
 VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
+/* The simulation that steps a batch's arena, for vlj_debug_set_graphs,
+ * vlj_debug_kernel_timing / _time and vlj_debug_kernels_executed only (it
+ * stays owned by the batch). */
+VLJ_API vlj_status vlj_debug_batch_sim(vlj_batch *batch, vlj_sim **sim);
 
 #ifdef __cplusplus
 }

@@ -51,10 +51,12 @@ vlj_status check_settings(const vlj_settings* st) {
 }
 
 // What LennardJones::new derives from the settings (lennard_jones.rs:450-560).
-// min_cells is 3 for the reference's 27-cell search.
+// min_cells is 3 for the reference's 27-cell search (lennard_jones.rs:457-461);
+// batched replicas accept 2, where the list build visits each distinct
+// neighbour cell once.
 vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3], double cutoff,
                     double skin, double dt, bool shifted_force, const vlj_thermostat& t,
-                    uint32_t profile_bins, Box& b) {
+                    uint32_t profile_bins, Box& b, uint32_t min_cells) {
     std::memset(&b, 0, sizeof b);
     const double list_radius = cutoff + skin;
     uint32_t cells[3];
@@ -64,9 +66,10 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
         double c = std::floor(b.box[k] / list_radius);
         cells[k] = c < 0.0 ? 0u : (c > 4.0e9 ? 4000000000u : (uint32_t)c);
     }
-    if (cells[0] < 3 || cells[1] < 3 || cells[2] < 3)
+    if (cells[0] < min_cells || cells[1] < min_cells || cells[2] < min_cells)
         return fail(VLJ_BOX_TOO_SMALL,
-                    "the box must be at least three (cutoff + skin) wide on every axis");
+                    "the box must be at least %s (cutoff + skin) wide on every axis",
+                    min_cells >= 3 ? "three" : "two");
     while ((uint64_t)cells[0] * cells[1] * cells[2] > (1u << 20)) {
         int longest = 0;
         for (int k = 1; k < 3; k++)
@@ -315,7 +318,7 @@ vlj_status vlj_create(const vlj_particle* particles, size_t count, const vlj_set
     s->shifted_force = settings->shifted_force != 0;
     vlj_status st = make_box(particles, count, settings->box_size, settings->cutoff,
                              settings->skin, settings->dt, s->shifted_force, settings->thermostat,
-                             settings->profile_bins, s->box);
+                             settings->profile_bins, s->box, 3);
     if (st != VLJ_OK) {
         delete s;
         return st;
@@ -746,19 +749,52 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     }
     Arena& a = s->arena;
     std::memset(&a, 0, sizeof a);
-    const uint32_t n = s->n;
+    // boxes own consecutive runs of slots and cells
+    const bool batched = !s->replicas.empty();
+    std::vector<Box> boxes = batched ? s->replicas : std::vector<Box>{s->box};
+    uint64_t slots = 0, cells = 0;
+    uint32_t cap = 0;
+    for (Box& b : boxes) {
+        b.first = (uint32_t)slots;
+        b.cell_base = (uint32_t)cells;
+        slots += b.n;
+        cells += b.total_cells;
+        cap = std::max(cap, b.capacity);
+    }
+    if (slots >= (1ull << 31)) return fail(VLJ_INVALID_ARG, "at most 2^31 - 1 particles in all");
+    if (cells >= (1ull << 32) - 1) return fail(VLJ_INVALID_ARG, "too many cells in all boxes");
+    if (batched)
+        s->replicas = boxes;
+    else
+        s->box = boxes[0];
+    const uint32_t n = (uint32_t)slots;
     const uint32_t seg = (n + 15u) / 16u * 16u;  // lennard_jones.rs:470
-    a.nboxes = 1;
+    s->n = n;
+    a.nboxes = (uint32_t)boxes.size();
     a.nslots = n;
     a.seg = seg;
-    a.ncells = s->box.total_cells;
-    s->box.first = 0;
-    s->box.cell_base = 0;
+    a.ncells = (uint32_t)cells;
     Box* d_box = nullptr;
-    TRY(dalloc(s, &d_box, 1));
+    TRY(dalloc(s, &d_box, boxes.size()));
     a.boxes = d_box;
-    TRY(dalloc(s, &a.ctrl, 1));
+    TRY(dalloc(s, &a.ctrl, boxes.size()));
     TRY(dalloc(s, &a.glob, 1));
+    if (batched) {
+        std::vector<uint32_t> of_slot(seg, 0u), of_cell(a.ncells);
+        for (uint32_t b = 0; b < a.nboxes; b++) {
+            std::fill(of_slot.begin() + boxes[b].first, of_slot.begin() + boxes[b].first + boxes[b].n, b);
+            std::fill(of_cell.begin() + boxes[b].cell_base,
+                      of_cell.begin() + boxes[b].cell_base + boxes[b].total_cells, b);
+        }
+        uint32_t *d_slot = nullptr, *d_cell = nullptr;
+        TRY(dalloc(s, &d_slot, seg));
+        TRY(dalloc(s, &d_cell, a.ncells));
+        CUDA_TRY(cudaMemcpy(d_slot, of_slot.data(), sizeof(uint32_t) * seg, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(d_cell, of_cell.data(), sizeof(uint32_t) * a.ncells,
+                            cudaMemcpyHostToDevice));
+        a.box_of_slot = d_slot;
+        a.box_of_cell = d_cell;
+    }
     TRY(dalloc(s, &a.x, 3 * (size_t)seg));
     TRY(dalloc(s, &a.v, 3 * (size_t)seg));
     TRY(dalloc(s, &a.id, seg));
@@ -772,22 +808,23 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));
     TRY(dalloc(s, &a.count, a.ncells));
     TRY(dalloc(s, &a.list_count, seg));
-    TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((s->box.capacity + 3) / 4)));
-    TRY(make_list_map(a, (s->box.capacity + 3) / 4, &s->list_map));
+    TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((cap + 3) / 4)));
+    TRY(dalloc(s, &a.block_rows, ((size_t)seg + kForceThreads - 1) / kForceThreads));
+    TRY(make_list_map(a, (cap + 3) / 4, &s->list_map));
     TRY(dalloc(s, &a.sx, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sv, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sid, seg));
     TRY(dalloc(s, &a.scell, seg));
-    TRY(dalloc(s, &a.accum, kSlots));
+    TRY(dalloc(s, &a.accum, (size_t)kSlots * boxes.size()));
     TRY(dalloc(s, &a.pe_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.w_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.vel4, seg));
     TRY(dalloc(s, &a.vcanon, 3 * (size_t)seg));
-    if (s->box.profile_bins)
+    if (!batched && s->box.profile_bins)
         TRY(dalloc(s, &a.profile, (size_t)s->box.profile_bins * 8 + 3));
-    // the last cell of the box ends at the last slot
+    // the last cell of the last box ends at the last slot
     CUDA_TRY(cudaMemcpy(a.cell_start + a.ncells, &n, sizeof n, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(d_box, &s->box, sizeof(Box), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_box, boxes.data(), sizeof(Box) * boxes.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMallocHost(&s->ring, sizeof(Readback) * kRing));
     CUDA_TRY(cudaMallocHost(&s->pin_x, sizeof(double) * 3 * (size_t)seg));
     CUDA_TRY(cudaMallocHost(&s->pin_v, sizeof(double) * 3 * (size_t)seg));

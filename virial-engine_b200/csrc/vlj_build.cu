@@ -48,6 +48,14 @@ __device__ __noinline__ bool ref_test(const Arena& a, const Box& bx, uint32_t i,
     return r2 < bx.list_r2;
 }
 
+// Whether stencil offset d (-1, 0, 1) along an axis of n cells reaches a cell
+// an earlier offset already did: with two cells -1 and +1 are the same
+// neighbour, with one cell every offset is the home cell. Boxes of three or
+// more cells (all the reference allows) visit all 27 cells.
+__device__ __forceinline__ bool repeats(int32_t d, int32_t n) {
+    return (n == 2 && d == 1) || (n == 1 && d != 0);
+}
+
 __global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
@@ -93,14 +101,17 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a
         uint32_t* wrow = a.list + (size_t)i * 4u;
         uint32_t wcol = 0;
         for (int32_t dz = -1; dz <= 1; dz++) {
+            if (repeats(dz, n[2])) continue;
             int32_t uz = c[2] + dz;
             uz = uz < 0 ? uz + n[2] : (uz >= n[2] ? uz - n[2] : uz);
             for (int32_t dy = -1; dy <= 1; dy++) {
+                if (repeats(dy, n[1])) continue;
                 int32_t uy = c[1] + dy;
                 uy = uy < 0 ? uy + n[1] : (uy >= n[1] ? uy - n[1] : uy);
                 const uint32_t row =
                     bx.cell_base + ((uint32_t)uz * (uint32_t)n[1] + (uint32_t)uy) * (uint32_t)n[0];
                 for (int32_t dx = -1; dx <= 1; dx++) {
+                    if (repeats(dx, n[0])) continue;
                     int32_t ux = c[0] + dx;
                     ux = ux < 0 ? ux + n[0] : (ux >= n[0] ? ux - n[0] : ux);
                     const uint32_t nc = row + (uint32_t)ux;
@@ -157,13 +168,19 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a
                 }
             }
         }
+        const uint32_t kept = found < cap ? found : cap;
         if (home) {
-            const uint32_t kept = found < cap ? found : cap;
             a.list_count[i] = kept;
             if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
             a.snap[i] = own_enc;
             longest = max(longest, kept);
         }
+        // rows each force block stages: one atomic per block these lanes
+        // touch (a cell's slots are mostly in one block after a reorder)
+        const uint32_t blk = home ? i / (uint32_t)kForceThreads : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, blk);
+        const uint32_t rows = __reduce_max_sync(peers, home ? (kept + 3u) / 4u : 0u);
+        if (home && lane == (uint32_t)(__ffs(peers) - 1)) atomicMax(&a.block_rows[blk], rows);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));

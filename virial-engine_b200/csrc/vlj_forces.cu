@@ -99,7 +99,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
                                                     bool valid, const uint4* __restrict__ cur) {
     PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u};
     const uint32_t first = blockIdx.x * kForceThreads;
-    const uint32_t rows = (a.glob->max_count + 3u) / 4u;
+    const uint32_t rows = a.block_rows[blockIdx.x];
     const uint32_t tiles = (rows + kTileRows - 1u) / kTileRows;
     if (threadIdx.x == 0) {
         for (int k = 0; k < kTileSlots; k++) bar_init(&st.bar[k]);
@@ -132,8 +132,15 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         s.ay -= dy * f;
         s.az -= dz * f;
         if (ENERGIES && in) {
+            // The sums take r^2 rounded once from the exact separation (the
+            // integer differences times the box step are exact in f64): on a
+            // lattice, where every pair at one distance rounds alike, the f32
+            // components' three roundings would bias the virial coherently.
+            const double ex = (double)(int32_t)(pj.x - own.x) * (double)dec0;
+            const double ey = (double)(int32_t)(pj.y - own.y) * (double)dec1;
+            const double ez = (double)(int32_t)(pj.z - own.z) * (double)dec2;
             float rf, u, t, e;
-            lj_pair<SHIFTED_FORCE>(r2, bx, rf, u);
+            lj_pair<SHIFTED_FORCE>((float)(ex * ex + ey * ey + ez * ez), bx, rf, u);
             two_sum(s.pe, 0.5f * u, t, e);
             s.pe = t;
             s.pe_lo += e;

@@ -107,7 +107,7 @@ struct Global {
     uint32_t fault;      // first error a kernel recorded (0 none)
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
-    uint32_t max_count;          // longest list built so far (rows the force kernels stage)
+    uint32_t max_count;          // longest list built so far
     uint32_t pad;
 };
 
@@ -140,6 +140,11 @@ struct Arena {
     uint32_t* count;
     uint32_t* list_count;
     uint32_t* list;
+    // per force block (kForceThreads slots): rows (four entries each) of the
+    // longest list in it, so a block stages only the rows its particles use. Reset at each rebuild of
+    // the box that holds the whole block; a block across two boxes keeps the
+    // largest value it ever had (more rows staged, never fewer).
+    uint32_t* block_rows;
     // reorder scratch
     double* sx;
     double* sv;
@@ -228,18 +233,20 @@ __device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, ui
     return make_uint4(c0, c1, c2, c3);
 }
 
-// r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545). The
-// reciprocal and square root are the hardware approximations (about 1 ulp),
-// well inside the f32 pair arithmetic's own error.
+// r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545), for the
+// energy and virial sums. The reciprocal and the square root are correctly
+// rounded: on a lattice every pair at one distance rounds the same way, so a
+// bias of a few ulp would add up coherently over all pairs, and the virial
+// (a difference of repulsive and attractive terms) would show it.
 template <bool SHIFTED_FORCE>
 __device__ __forceinline__ void lj_pair(float r2, const Box& b, float& rf, float& u) {
-    float inv2 = __fdividef(1.0f, r2);
+    float inv2 = __frcp_rn(r2);
     float s6 = inv2 * inv2 * inv2;
     float s12 = s6 * s6;
     rf = 24.0f * (2.0f * s12 - s6);
     u = 4.0f * (s12 - s6) - b.shift;
     if (SHIFTED_FORCE) {
-        float r = r2 * rsqrtf(r2);
+        float r = __fsqrt_rn(r2);
         rf -= r * b.force_shift;
         u += (r - b.rc) * b.force_shift;
     }

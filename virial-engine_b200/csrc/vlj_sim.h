@@ -25,7 +25,7 @@ double scale_for(double magnitude);
 vlj_status check_settings(const vlj_settings* st);
 vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3], double cutoff,
                     double skin, double dt, bool shifted_force, const vlj_thermostat& t,
-                    uint32_t profile_bins, Box& b);
+                    uint32_t profile_bins, Box& b, uint32_t min_cells);
 
 }  // namespace vlj
 
@@ -37,6 +37,8 @@ struct vlj_sim {
     uint32_t n = 0;
     bool shifted_force = false;
     vlj::Box box{};
+    // batched: one Box per replica, in slot order (empty for a single box)
+    std::vector<vlj::Box> replicas;
     vlj::Arena arena{};
     CUtensorMap list_map;  // list rows for the force kernels' TMA tiles
     std::vector<void*> allocations;

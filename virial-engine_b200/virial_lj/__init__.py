@@ -28,7 +28,7 @@ _lib = _ffi.load()
 __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
-    "lattice_fcc", "particles", "device_count", "library_path", "launches",
+    "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
 ]
 
 
@@ -515,6 +515,37 @@ class Batch:
         _check(_lib.vlj_batch_read_particles(self._h, int(replica), _ffi.ptr(out)))
         return out
 
+    def run(self, steps):
+        """Step, then wait for the steps to finish."""
+        _check(_lib.vlj_batch_run(self._h, int(steps)))
+
+    def box_size(self, replica):
+        out = (C.c_double * 3)()
+        _check(_lib.vlj_batch_box_size(self._h, int(replica), out))
+        return list(out)
+
+    # inspection and timing, through the simulation that steps the arena
+    def _sim(self):
+        h = C.c_void_p()
+        _check(_lib.vlj_debug_batch_sim(self._h, C.byref(h)))
+        return h
+
+    def set_graphs(self, on):
+        _check(_lib.vlj_debug_set_graphs(self._sim(), int(bool(on))))
+
+    def kernel_timing(self, on):
+        _check(_lib.vlj_debug_kernel_timing(self._sim(), int(bool(on))))
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_uint64()
+        _check(_lib.vlj_debug_kernel_time(self._sim(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def kernels_executed(self):
+        n = C.c_uint64()
+        _check(_lib.vlj_debug_kernels_executed(self._sim(), C.byref(n)))
+        return n.value
+
 
 # ---- host helpers (lennard_jones.rs:1377-1441) ----
 
@@ -539,3 +570,35 @@ def lattice_fcc(cells, density, temperature, seed):
     _check(_lib.vlj_lattice_fcc(int(cells), float(density), float(temperature), int(seed),
                                 _ffi.ptr(out), C.byref(box)))
     return out, box.value
+
+
+def uneven_replicas(count=512, seed=2024, sizes=(500, 20000), densities=(0.01, 0.90),
+                    temperatures=(0.7, 2.0), friction=1.0):
+    """Replicas of uneven size, density and temperature from one seed.
+
+    Replica r draws, from a xorshift64 stream (the reference's generator,
+    lennard_jones.rs:1410-1415), N log-uniform in `sizes`, density and
+    temperature uniform in their ranges; its box is the cube of side
+    (N / density)^(1/3) holding lattice(N, side, T, seed + r), under a
+    Langevin thermostat at T (friction `friction`, noise seed seed + r).
+    """
+    mask = (1 << 64) - 1
+    s = seed | 1
+
+    def uniform():
+        nonlocal s
+        s ^= (s << 13) & mask
+        s ^= s >> 7
+        s ^= (s << 17) & mask
+        return ((s >> 11) + 0.5) / float(1 << 53)
+
+    out = []
+    for r in range(int(count)):
+        n = int(round(math.exp(math.log(sizes[0]) + uniform() *
+                               (math.log(sizes[1]) - math.log(sizes[0])))))
+        rho = densities[0] + uniform() * (densities[1] - densities[0])
+        t = temperatures[0] + uniform() * (temperatures[1] - temperatures[0])
+        side = (n / rho) ** (1.0 / 3.0)
+        p = lattice(n, side, t, seed + r)
+        out.append(Replica(p, [side] * 3, Langevin(t, friction, (seed + r) & 0xFFFFFFFF)))
+    return out

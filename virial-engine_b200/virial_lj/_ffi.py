@@ -103,6 +103,9 @@ SIGNATURES = {
     "vlj_batch_measure": [_vp, _P(Measurement)],
     "vlj_batch_read_particles": [_vp, C.c_size_t, _vp],
     "vlj_batch_count": [_vp, _P(C.c_size_t), _P(C.c_uint64)],
+    "vlj_batch_run": [_vp, C.c_uint64],
+    "vlj_batch_box_size": [_vp, C.c_size_t, _P(C.c_double)],
+    "vlj_debug_batch_sim": [_vp, _P(_vp)],
     "vlj_debug_grid_info": [_vp, _P(GridInfo)],
     "vlj_debug_read_grid": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "vlj_debug_force_rebuild": [_vp],
