@@ -50,6 +50,12 @@ FALLBACK_HBM_GBS = 6650.0
 ALGO_BYTES = 96          # f64 x and v read + written per particle-step
 
 
+BATCH = dict(replicas=512, seed=2024, sizes=(500, 20000), densities=(0.01, 0.90),
+             temperatures=(0.7, 2.0), friction=1.0, dt=0.004, cutoff=2.5, skin=0.3)
+PLAIN_SAMPLE_EVERY = 16  # plain-path comparison: every 16th replica as its own simulation
+PLAIN_SAMPLE_STEPS = 50
+
+
 def config(n, world):
     return {
         "workload": "lj-fcc40x4-256k-rho0.8442-shifted-force-langevin",
@@ -61,13 +67,15 @@ def config(n, world):
     }
 
 
-def flops_per_particle_step(density):
-    """Algorithmic f32 flops: 11 per list candidate, 26 per force-shifted pair
-    inside the cutoff (FMA = 2)."""
+def flops_per_particle_step(density, per_pair=26.0, cutoff=None, skin=None):
+    """Algorithmic f32 flops: 11 per list candidate, 26 per force-shifted
+    (20 per truncated-shifted) pair inside the cutoff (FMA = 2)."""
     import math
-    n_list = 4.0 / 3.0 * math.pi * (WORK["cutoff"] + WORK["skin"]) ** 3 * density
-    n_rc = 4.0 / 3.0 * math.pi * WORK["cutoff"] ** 3 * density
-    return 11.0 * n_list + 26.0 * n_rc
+    rc = WORK["cutoff"] if cutoff is None else cutoff
+    sk = WORK["skin"] if skin is None else skin
+    n_list = 4.0 / 3.0 * math.pi * (rc + sk) ** 3 * density
+    n_rc = 4.0 / 3.0 * math.pi * rc ** 3 * density
+    return 11.0 * n_list + per_pair * n_rc
 
 
 def measured_peaks():
@@ -89,7 +97,7 @@ def profile_traffic():
 
 
 class Clocks:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """nvidia-smi samples every 100 ms while the timed regions run."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -103,7 +111,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -208,6 +216,105 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
+    """512 replicas of uneven N, density and temperature in one arena: the
+    batched form, timed like the plain box, then the same replicas (a
+    sample) each run as a plain single-box simulation, back to back."""
+    import torch
+    import virial_lj as vl
+
+    reps = vl.uneven_replicas(BATCH["replicas"], BATCH["seed"] + 7919 * rank, BATCH["sizes"],
+                              BATCH["densities"], BATCH["temperatures"], BATCH["friction"])
+    total = sum(len(r.particles) for r in reps)
+    b = vl.Batch(reps, cutoff=BATCH["cutoff"], skin=BATCH["skin"], dt=BATCH["dt"],
+                 stream=stream.cuda_stream)
+    b.step(max(args.warmup, 3))
+    stream.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k0 = b.kernels_executed()
+    barrier(world)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush_l2()
+        starts[k].record(stream)
+        b.step(1)
+        ends[k].record(stream)
+    stream.synchronize()
+    barrier(world)
+    launches = b.kernels_executed() - k0
+    total_ms = sum(x.elapsed_time(y) for x, y in zip(starts, ends))
+    max_ms = reduce_max(world, total_ms)
+    value = world * total * args.steps / (max_ms / 1e3)
+    # step kernel alone
+    b.kernel_timing(True)
+    for k in range(args.steps):
+        flush_l2()
+        b.step(1)
+    kern_ms, kern_n = b.kernel_time()
+    b.kernel_timing(False)
+    kern_s = kern_ms / 1e3 / max(kern_n, 1)
+    ms = b.measure()
+    b.close()
+    # rooflines with each replica's own density (truncated-shifted pairs)
+    dens = [len(r.particles) / (r.box_size[0] * r.box_size[1] * r.box_size[2]) for r in reps]
+    flops = sum(len(r.particles) * flops_per_particle_step(d, 20.0, BATCH["cutoff"], BATCH["skin"])
+                for r, d in zip(reps, dens))
+    bytes_ = ALGO_BYTES * total
+    bound_s = max(bytes_ / (hbm_peak * 1e9), flops / (fp32_peak * 1e12)) if fp32_peak else None
+
+    # the plain path on the same replicas: every PLAIN_SAMPLE_EVERY-th replica
+    # as its own simulation, one after another (as the reference would run them)
+    plain_n, plain_s = 0, 0.0
+    for r in reps[::PLAIN_SAMPLE_EVERY]:
+        st = vl.Settings(r.box_size, cutoff=BATCH["cutoff"], dt=BATCH["dt"],
+                         thermostat=r.thermostat, skin=BATCH["skin"])
+        try:
+            sim = vl.LennardJones(r.particles, st, stream=stream.cuda_stream)
+        except vl.VljError:
+            continue  # a box under three cells wide: the plain path refuses it
+        sim.step(3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream.synchronize()
+        e0.record(stream)
+        sim.step(PLAIN_SAMPLE_STEPS)
+        e1.record(stream)
+        stream.synchronize()
+        plain_s += e0.elapsed_time(e1) / 1e3
+        plain_n += len(r.particles) * PLAIN_SAMPLE_STEPS
+        sim.close()
+    plain_value = plain_n / plain_s if plain_s else None
+    # compressibility factor at the measured temperature: PV / NkT = 1 + W / (2 KE)
+    pv = [1.0 + m.virial / (2.0 * m.kinetic) for m in ms]
+    return {
+        "workload": f"lj-batched-{BATCH['replicas']}-replicas-uneven",
+        "value": value, "unit": UNIT, "ms_per_step": max_ms / args.steps, "steps": args.steps,
+        "replicas": len(reps), "particles": total,
+        "config": {"sizes": "N log-uniform in [500, 20000]", "densities": "uniform in [0.01, 0.90]",
+                   "temperatures": "uniform in [0.7, 2.0], Langevin gamma=1.0",
+                   "cutoff": BATCH["cutoff"], "cutoff_style": "truncated-shifted",
+                   "skin": BATCH["skin"], "dt": BATCH["dt"],
+                   "seed": BATCH["seed"] + 7919 * rank,
+                   "l2": "flushed between timed steps (256 MiB write on the stream)"},
+        "gpu_launches": launches,
+        "step_kernel_us": kern_s * 1e6,
+        "roofline": {"hbm_achieved_gbs": bytes_ / kern_s / 1e9, "hbm_peak_gbs": hbm_peak,
+                     "hbm_frac": bytes_ / kern_s / 1e9 / hbm_peak,
+                     "fp32_achieved_tflops": flops / kern_s / 1e12, "fp32_peak_tflops": fp32_peak,
+                     "fp32_frac": flops / kern_s / 1e12 / fp32_peak if fp32_peak else None,
+                     "bound_us": bound_s * 1e6 if bound_s else None,
+                     "frac": bound_s / kern_s if bound_s else None,
+                     "kernel": "step_kernel<false>",
+                     "flops_per_step": flops, "algorithmic_bytes_per_step": bytes_},
+        "plain_same_replicas": {"value": plain_value, "unit": UNIT,
+                                "sample": f"every {PLAIN_SAMPLE_EVERY}th replica as its own "
+                                          f"simulation, {PLAIN_SAMPLE_STEPS} steps each, back "
+                                          "to back (CUDA events)"},
+        "batched_vs_plain": value / plain_value if plain_value else None,
+        "pv_over_nkt": {"min": min(pv), "max": max(pv)},
+    }
+
+
 def run_ours(args, world, rank, gpu_index):
     import numpy as np
     import torch
@@ -254,7 +361,6 @@ def run_ours(args, world, rank, gpu_index):
     stream.synchronize()
     barrier(world)
     torch.cuda.synchronize()
-    clk = clocks.stop() if rank == 0 else None
     total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     launches = sim.kernels_executed() - k0  # this library's kernels that ran in the region
     m = sim.measure_now()
@@ -276,6 +382,10 @@ def run_ours(args, world, rank, gpu_index):
     fpps = flops_per_particle_step(WORK["density"])
     fp32_achieved = fpps * n / avg_kernel_s / 1e12
     traffic = profile_traffic()
+
+    # ---- the batched form on 512 uneven replicas, and the plain path on them ----
+    batched = run_batched(args, world, rank, stream, flush_l2, peak, fp32_peak)
+    clk = clocks.stop() if rank == 0 else None
 
     # ---- end to end through the C ABI with host buffers ----
     e2e_steps = max(3, min(args.steps, 10))
@@ -325,6 +435,7 @@ def run_ours(args, world, rank, gpu_index):
                               "flops_per_particle_step": fpps,
                               "peak_source": "measured live (FMA chains on every SM)"},
             "cpu_baseline": cpu,
+            "batched": batched,
             "clocks": clk,
             "gpu_launches": launches,
             "list_rebuilds_timed": rebuilds,
