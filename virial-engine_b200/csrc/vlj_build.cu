@@ -6,17 +6,24 @@
 // reference's f32 test on packed positions, operation for operation, so the
 // lists are the reference's entry for entry.
 //
-// One warp serves one home cell: up to 32 home particles, one per lane. For
-// each neighbour cell in stencil order the warp copies the cell's candidates
-// (slot and encoded position) into shared memory once, then every lane tests
-// its home particle against each candidate in turn -- the same candidates in
-// the same order for all lanes, so the warp never diverges on the stream and
-// the inner loop reads only shared memory. A test on the 32-bit encoded
-// positions settles every candidate farther than sqrt(prefilter_r2) (out) or
-// nearer than sqrt(accept_r2) (in); the two radii bracket list_r2 by more
-// than the reference's f32 separations and the encoded ones can differ, so
-// only candidates in the thin shell between them need the reference's own
-// arithmetic.
+// A warp serves one home cell at a time: up to 32 home particles, one per
+// lane. The grid is resident at once (kBuildBlocksPerSM blocks per SM) and
+// its warps take the non-empty cells of the rebuilding boxes from the step's
+// work list, so boxes that do not rebuild and empty cells cost nothing. The
+// warp reads the 27 neighbour cells' ranges at once (a lane each), which makes
+// the cells' candidates one stream in stencil order; it fetches the stream
+// kRound candidates at a time (slot, then encoded position, all loads of a
+// round in flight together), copies those within reach of the home cell into
+// shared memory, then every lane tests its home particle against each staged
+// candidate in turn -- the same candidates in the same order for all lanes, so
+// the warp never diverges on the stream and the inner loop reads only shared
+// memory. A dense home cell costs a few rounds of two dependent loads.
+//
+// A test on the 32-bit encoded positions settles every candidate farther than
+// sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in); the two radii
+// bracket list_r2 by more than the reference's f32 separations and the encoded
+// ones can differ, so only candidates in the thin shell between them need the
+// reference's own arithmetic.
 #include <cuda_runtime.h>
 
 #include "vlj_device.cuh"
@@ -24,7 +31,12 @@
 
 namespace vlj {
 
-constexpr int kBuildWarps = 8;  // home cells per block
+constexpr int kBuildWarps = 8;  // warps per block, each building one home cell at a time
+constexpr int kRound = 128;     // candidates a warp fetches and stages per round
+#ifndef VLJ_BUILD_BLOCKS_PER_SM
+#define VLJ_BUILD_BLOCKS_PER_SM 3
+#endif
+constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;  // register budget of the build
 
 // The reference's predicate for slots i and j: nearest((pj.hi - xh) +
 // (unpack(pj) - xl)), squared length < list_r2, in f32 as written
@@ -56,131 +68,170 @@ __device__ __forceinline__ bool repeats(int32_t d, int32_t n) {
     return (n == 2 && d == 1) || (n == 1 && d != 0);
 }
 
-__global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a) {
+__global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_list_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
     __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
-    __shared__ uint32_t s_j[kBuildWarps][32];
-    __shared__ uint4 s_enc[kBuildWarps][32];
+    __shared__ uint32_t s_j[kBuildWarps][kRound];
+    __shared__ uint4 s_enc[kBuildWarps][kRound];
     for (int t = threadIdx.x; t < 512; t += blockDim.x)
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t cell = blockIdx.x * kBuildWarps + warp;
-    if (cell >= a.ncells) return;  // whole warps leave together
-    const uint32_t b = box_of_cell(a, cell);
-    if (!rebuilding(a, b)) return;
-    const Box& bx = a.boxes[b];
-    const uint4* __restrict__ cur = a.cache[a.glob->phase];
-    const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
-    const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};
-    const int32_t ci = (int32_t)(cell - bx.cell_base);
-    const int32_t c[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
-    const uint32_t cap = bx.capacity;
-    const float pre_r2 = bx.prefilter_r2, acc_r2 = bx.accept_r2;
-    // The home cell as an interval of encoded coordinates per axis, for the
-    // staging filter: a candidate farther than reach_r2 from the whole home
-    // cell cannot be in any home particle's list.
-    uint32_t home_lo[3], home_w[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        home_lo[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)c[k] * (double)bx.cell_size_f[k] * bx.enc[k]);
-        home_w[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)bx.cell_size_f[k] * bx.enc[k]);
-    }
-    const float reach_r2 = bx.reach_r2;
-    const size_t row_stride = (size_t)a.seg * 4u;
-    const unsigned below = (1u << lane) - 1u;
+    // Warps take home cells from the step's work list (the non-empty cells of
+    // the boxes that rebuild) until it runs out.
+    const uint32_t cells = a.glob->work_cells;
     uint32_t longest = 0;
-    const uint32_t hbeg = a.cell_start[cell], hend = a.cell_start[cell + 1];
-    for (uint32_t h0 = hbeg; h0 < hend; h0 += 32) {
-        const bool home = h0 + lane < hend;
-        const uint32_t i = home ? a.sorted[h0 + lane] : 0u;
-        const uint4 own_enc = home ? cur[i] : make_uint4(0u, 0u, 0u, 0u);
-        uint32_t found = 0;
-        // where the next entry goes: row (found / 4), column (found % 4)
-        uint32_t* wrow = a.list + (size_t)i * 4u;
-        uint32_t wcol = 0;
-        for (int32_t dz = -1; dz <= 1; dz++) {
-            if (repeats(dz, n[2])) continue;
-            int32_t uz = c[2] + dz;
-            uz = uz < 0 ? uz + n[2] : (uz >= n[2] ? uz - n[2] : uz);
-            for (int32_t dy = -1; dy <= 1; dy++) {
-                if (repeats(dy, n[1])) continue;
-                int32_t uy = c[1] + dy;
-                uy = uy < 0 ? uy + n[1] : (uy >= n[1] ? uy - n[1] : uy);
-                const uint32_t row =
-                    bx.cell_base + ((uint32_t)uz * (uint32_t)n[1] + (uint32_t)uy) * (uint32_t)n[0];
-                for (int32_t dx = -1; dx <= 1; dx++) {
-                    if (repeats(dx, n[0])) continue;
-                    int32_t ux = c[0] + dx;
-                    ux = ux < 0 ? ux + n[0] : (ux >= n[0] ? ux - n[0] : ux);
-                    const uint32_t nc = row + (uint32_t)ux;
-                    const uint32_t nend = a.cell_start[nc + 1];
-                    for (uint32_t c0 = a.cell_start[nc]; c0 < nend; c0 += 32) {
-                        // stage up to 32 candidates of this cell, keeping (in
-                        // order) those within reach of the home cell
-                        uint32_t j = 0;
-                        uint4 pe = make_uint4(0u, 0u, 0u, 0u);
-                        bool keep = false;
-                        if (c0 + lane < nend) {
-                            j = a.sorted[c0 + lane];
-                            pe = __ldg(cur + j);
-                            float g2 = 0.0f;
-#pragma unroll
-                            for (int k = 0; k < 3; k++) {
-                                // periodic gap between the candidate and the
-                                // interval [lo, lo + w): above it, or below it
-                                // around the box, whichever is shorter
-                                const uint32_t w = k == 0 ? pe.x : (k == 1 ? pe.y : pe.z);
-                                const uint32_t off = w - home_lo[k];
-                                const uint32_t gap =
-                                    off < home_w[k] ? 0u : min(off - home_w[k], 0u - off);
-                                const float g = (float)gap * dec[k];
-                                g2 += g * g;
-                            }
-                            keep = g2 < reach_r2;
-                        }
-                        const unsigned kept_mask = __ballot_sync(0xffffffffu, keep);
-                        if (keep) {
-                            const uint32_t at = (uint32_t)__popc(kept_mask & below);
-                            s_j[warp][at] = j;
-                            s_enc[warp][at] = pe;
-                        }
-                        __syncwarp();
-                        const uint32_t m = (uint32_t)__popc(kept_mask);
-                        for (uint32_t q = 0; q < m; q++) {
-                            const uint32_t jq = s_j[warp][q];
-                            const float r2e = encoded_r2(s_enc[warp][q], own_enc, dec);
-                            bool in = r2e < acc_r2;
-                            if (!in && r2e < pre_r2 && home && jq != i) in = ref_test(a, bx, i, jq, s_q510);
-                            if (in && home && jq != i) {
-                                if (found < cap) wrow[wcol] = jq;
-                                found += 1;
-                                wcol += 1;
-                                if (wcol == 4u) {
-                                    wcol = 0;
-                                    wrow += row_stride;
-                                }
-                            }
-                        }
-                        __syncwarp();
-                    }
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&a.glob->next_build, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= cells) break;
+        const uint32_t cell = a.work[t];
+        const uint32_t b = box_of_cell(a, cell);
+        const uint32_t hbeg = a.cell_start[cell], hend = a.cell_start[cell + 1];
+        const Box& bx = a.boxes[b];
+        const uint4* __restrict__ cur = a.cache[a.glob->phase];
+        const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
+        const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};
+        const int32_t ci = (int32_t)(cell - bx.cell_base);
+        const int32_t c[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+        const uint32_t cap = bx.capacity;
+        const float pre_r2 = bx.prefilter_r2, acc_r2 = bx.accept_r2;
+
+        // Lane s < 27 takes stencil cell s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1),
+        // so lane order is the reference's order; its candidates are
+        // sorted[cs, cs + cnt), at offset off in the stream of all of them.
+        uint32_t cs = 0, cnt = 0;
+        if (lane < 27u) {
+            const int32_t d[3] = {(int32_t)(lane % 3u) - 1, (int32_t)((lane / 3u) % 3u) - 1,
+                                  (int32_t)(lane / 9u) - 1};
+            if (!repeats(d[0], n[0]) && !repeats(d[1], n[1]) && !repeats(d[2], n[2])) {
+                int32_t u[3];
+    #pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    u[k] = c[k] + d[k];
+                    u[k] = u[k] < 0 ? u[k] + n[k] : (u[k] >= n[k] ? u[k] - n[k] : u[k]);
                 }
+                const uint32_t nc = bx.cell_base +
+                    ((uint32_t)u[2] * (uint32_t)n[1] + (uint32_t)u[1]) * (uint32_t)n[0] + (uint32_t)u[0];
+                cs = a.cell_start[nc];
+                cnt = a.cell_start[nc + 1] - cs;
             }
         }
-        const uint32_t kept = found < cap ? found : cap;
-        if (home) {
-            a.list_count[i] = kept;
-            if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
-            a.snap[i] = own_enc;
-            longest = max(longest, kept);
+        uint32_t off = cnt;
+    #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= (uint32_t)o) off += t;
         }
-        // rows each force block stages: one atomic per block these lanes
-        // touch (a cell's slots are mostly in one block after a reorder)
-        const uint32_t blk = home ? i / (uint32_t)kForceThreads : 0xffffffffu;
-        const unsigned peers = __match_any_sync(0xffffffffu, blk);
-        const uint32_t rows = __reduce_max_sync(peers, home ? (kept + 3u) / 4u : 0u);
-        if (home && lane == (uint32_t)(__ffs(peers) - 1)) atomicMax(&a.block_rows[blk], rows);
+        const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+        off -= cnt;  // exclusive; lanes 27..31 sit at `total`
+
+        // The home cell as an interval of encoded coordinates per axis, for the
+        // staging filter: a candidate farther than reach_r2 from the whole home
+        // cell cannot be in any home particle's list.
+        uint32_t home_lo[3], home_w[3];
+    #pragma unroll
+        for (int k = 0; k < 3; k++) {
+            home_lo[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)c[k] * (double)bx.cell_size_f[k] * bx.enc[k]);
+            home_w[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)bx.cell_size_f[k] * bx.enc[k]);
+        }
+        const float reach_r2 = bx.reach_r2;
+        const size_t row_stride = (size_t)a.seg * 4u;
+        const unsigned below = (1u << lane) - 1u;
+        for (uint32_t h0 = hbeg; h0 < hend; h0 += 32) {
+            const bool home = h0 + lane < hend;
+            const uint32_t i = home ? a.sorted[h0 + lane] : 0u;
+            const uint4 own_enc = home ? cur[i] : make_uint4(0u, 0u, 0u, 0u);
+            uint32_t found = 0;
+            // where the next entry goes: row (found / 4), column (found % 4)
+            uint32_t* wrow = a.list + (size_t)i * 4u;
+            uint32_t wcol = 0;
+            for (uint32_t base = 0; base < total; base += kRound) {
+                // Fetch the next kRound candidates of the stream (kRound / 32 per
+                // lane, loads in flight together), keep those within reach of the
+                // home cell, and stage them in stream order.
+                uint32_t j[kRound / 32];
+    #pragma unroll
+                for (int r = 0; r < kRound / 32; r++) {
+                    const uint32_t t = base + (uint32_t)r * 32u + lane;
+                    // the last stencil lane whose stream offset is <= t (all
+                    // lanes search, past-the-end ones for the last candidate)
+                    const uint32_t tt = t < total ? t : total - 1u;
+                    uint32_t lo = 0, hi = 32;
+    #pragma unroll
+                    for (int q = 0; q < 5; q++) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (__shfl_sync(0xffffffffu, off, mid) <= tt) lo = mid; else hi = mid;
+                    }
+                    const uint32_t from = __shfl_sync(0xffffffffu, cs, lo);
+                    const uint32_t at = __shfl_sync(0xffffffffu, off, lo);
+                    j[r] = t < total ? a.sorted[from + t - at] : 0xffffffffu;
+                }
+                uint4 pe[kRound / 32];
+    #pragma unroll
+                for (int r = 0; r < kRound / 32; r++)
+                    pe[r] = j[r] != 0xffffffffu ? __ldg(cur + j[r]) : make_uint4(0u, 0u, 0u, 0u);
+                uint32_t staged = 0;
+    #pragma unroll
+                for (int r = 0; r < kRound / 32; r++) {
+                    bool keep = false;
+                    if (j[r] != 0xffffffffu) {
+                        float g2 = 0.0f;
+    #pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            // periodic gap between the candidate and the interval
+                            // [lo, lo + w): above it, or below it around the box,
+                            // whichever is shorter
+                            const uint32_t w = k == 0 ? pe[r].x : (k == 1 ? pe[r].y : pe[r].z);
+                            const uint32_t o = w - home_lo[k];
+                            const uint32_t gap = o < home_w[k] ? 0u : min(o - home_w[k], 0u - o);
+                            const float g = (float)gap * dec[k];
+                            g2 += g * g;
+                        }
+                        keep = g2 < reach_r2;
+                    }
+                    const unsigned kept_mask = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const uint32_t to = staged + (uint32_t)__popc(kept_mask & below);
+                        s_j[warp][to] = j[r];
+                        s_enc[warp][to] = pe[r];
+                    }
+                    staged += (uint32_t)__popc(kept_mask);
+                }
+                __syncwarp();
+                for (uint32_t q = 0; q < staged; q++) {
+                    const uint32_t jq = s_j[warp][q];
+                    const float r2e = encoded_r2(s_enc[warp][q], own_enc, dec);
+                    bool in = r2e < acc_r2;
+                    if (!in && r2e < pre_r2 && home && jq != i) in = ref_test(a, bx, i, jq, s_q510);
+                    if (in && home && jq != i) {
+                        if (found < cap) wrow[wcol] = jq;
+                        found += 1;
+                        wcol += 1;
+                        if (wcol == 4u) {
+                            wcol = 0;
+                            wrow += row_stride;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            const uint32_t kept = found < cap ? found : cap;
+            if (home) {
+                a.list_count[i] = kept;
+                if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
+                a.snap[i] = own_enc;
+                longest = max(longest, kept);
+            }
+            // rows each force block stages: one atomic per block these lanes
+            // touch (a cell's slots are mostly in one block after a reorder)
+            const uint32_t blk = home ? i / (uint32_t)kForceThreads : 0xffffffffu;
+            const unsigned peers = __match_any_sync(0xffffffffu, blk);
+            const uint32_t rows = __reduce_max_sync(peers, home ? (kept + 3u) / 4u : 0u);
+            if (home && lane == (uint32_t)(__ffs(peers) - 1)) atomicMax(&a.block_rows[blk], rows);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
@@ -188,7 +239,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, 4) build_list_kernel(Arena a
 }
 
 cudaError_t launch_build_list(const Arena& a, cudaStream_t s) {
-    build_list_kernel<<<blocks_for(a.ncells, kBuildWarps), kBuildWarps * 32, 0, s>>>(a);
+    build_list_kernel<<<(unsigned)sm_count() * kBuildBlocksPerSM, kBuildWarps * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 

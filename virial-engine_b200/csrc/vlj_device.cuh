@@ -13,6 +13,9 @@ inline unsigned blocks_for(uint64_t n, int threads = kBlock) {
     return b ? (unsigned)b : 1u;
 }
 cudaError_t after_launch(unsigned n = 1);
+// Streaming multiprocessors of the current device (cached per device): the
+// grid of the kernels that loop over the step's work list.
+int sm_count();
 cudaError_t launch_build_list(const Arena& a, cudaStream_t s);  // vlj_build.cu
 
 __device__ __forceinline__ uint32_t box_of_slot(const Arena& a, uint32_t slot) {

@@ -18,6 +18,19 @@ namespace vlj {
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long launches() { return g_launches.load(); }
 
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
 cudaError_t after_launch(unsigned n) {
     g_launches += n;
     return cudaGetLastError();
@@ -49,6 +62,8 @@ __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
     Global* g = a.glob;
     if (threadIdx.x == 0) {
         s_any = 0;
+        g->work_cells = 0u;
+        g->next_build = 0u;
         if (g->pending) {
             g->phase ^= 1u;
             g->step += 1ull;
@@ -110,6 +125,8 @@ __global__ void bin_kernel(Arena a) {
 
 // ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
 // the counts offset by the box's first slot; counts become zeroed cursors.
+// The box's non-empty cells join the step's work list for the sort and the
+// list build.
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 
@@ -163,6 +180,22 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
             }
             before += v[q];
         }
+        // append the non-empty cells to the work list: one atomic per warp
+        uint32_t nz = 0;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) nz += v[q] ? 1u : 0u;
+        uint32_t nz_incl = nz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, nz_incl, o);
+            if (lane >= o) nz_incl += t;
+        }
+        uint32_t at = 0;
+        if (lane == 31 && nz_incl) at = atomicAdd(&a.glob->work_cells, nz_incl);
+        at = __shfl_sync(0xffffffffu, at, 31) + nz_incl - nz;
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++)
+            if (v[q]) a.work[at++] = base + tile + threadIdx.x * kScanPer + q;
         __syncthreads();
         if (threadIdx.x == 0) s_carry += s_warp[kScanThreads / 32 - 1];
         __syncthreads();
@@ -181,9 +214,10 @@ __global__ void scatter_kernel(Arena a) {
 }
 
 // ---- per-cell order (grid.wgsl:129-148) ----
-// One warp per cell: each slot's rank is the number of smaller slots in the
-// cell, so the cell ends up sorted by slot index whatever order the scatter's
-// atomics produced. With reorder, every particle is also copied to the slot
+// A warp per cell of the step's work list (the resident grid's warps stride
+// through it): each slot's rank is the number of smaller slots in the cell, so
+// the cell ends up sorted by slot index whatever order the scatter's atomics
+// produced. With reorder, every particle is also copied to the slot
 // it takes in cell order (lennard_jones.wgsl:419-433).
 constexpr int kSortRegs = 8;  // cells up to 256 particles rank in registers
 
@@ -201,53 +235,56 @@ __device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, u
 __global__ void sort_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
-    uint32_t cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (cell >= a.ncells) return;
-    uint32_t b = box_of_cell(a, cell);
-    if (!rebuilding(a, b)) return;
-    const bool reorder = a.ctrl[b].reorder != 0u;
-    const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
-    const uint32_t m = end - start;
-    if (lane == 0) a.count[cell] = 0u;
-    if (m <= 32u * kSortRegs) {
-        uint32_t key[kSortRegs], rank[kSortRegs];
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t cells = a.glob->work_cells;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cells; w += warps) {
+        const uint32_t cell = a.work[w];
+        const uint32_t b = box_of_cell(a, cell);
+        const bool reorder = a.ctrl[b].reorder != 0u;
+        const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
+        const uint32_t m = end - start;
+        if (lane == 0) a.count[cell] = 0u;
+        if (m <= 32u * kSortRegs) {
+            uint32_t key[kSortRegs], rank[kSortRegs];
 #pragma unroll
-        for (int r = 0; r < kSortRegs; r++) {
-            uint32_t t = r * 32 + lane;
-            key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
-            rank[r] = 0;
-        }
-        for (int rr = 0; rr < kSortRegs; rr++) {
-            if ((uint32_t)rr * 32u >= m) break;
-            for (int src = 0; src < 32; src++) {
-                uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
-#pragma unroll
-                for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
+            for (int r = 0; r < kSortRegs; r++) {
+                uint32_t t = r * 32 + lane;
+                key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
+                rank[r] = 0;
             }
+            for (int rr = 0; rr < kSortRegs; rr++) {
+                if ((uint32_t)rr * 32u >= m) break;
+                for (int src = 0; src < 32; src++) {
+                    uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
+#pragma unroll
+                    for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < kSortRegs; r++) {
+                uint32_t t = r * 32 + lane;
+                if (t < m) {
+                    a.sorted[start + rank[r]] = key[r];
+                    if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
+                }
+            }
+        } else if (lane == 0) {
+            // insertion sort, as the reference, for improbably full cells
+            for (uint32_t s = start + 1; s < end; s++) {
+                uint32_t key = a.sorted[s];
+                uint32_t t = s;
+                while (t > start && a.sorted[t - 1] > key) {
+                    a.sorted[t] = a.sorted[t - 1];
+                    t -= 1;
+                }
+                a.sorted[t] = key;
+            }
+            if (reorder)
+                for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
         }
         __syncwarp();
-#pragma unroll
-        for (int r = 0; r < kSortRegs; r++) {
-            uint32_t t = r * 32 + lane;
-            if (t < m) {
-                a.sorted[start + rank[r]] = key[r];
-                if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
-            }
-        }
-    } else if (lane == 0) {
-        // insertion sort, as the reference, for improbably full cells
-        for (uint32_t s = start + 1; s < end; s++) {
-            uint32_t key = a.sorted[s];
-            uint32_t t = s;
-            while (t > start && a.sorted[t - 1] > key) {
-                a.sorted[t] = a.sorted[t - 1];
-                t -= 1;
-            }
-            a.sorted[t] = key;
-        }
-        if (reorder)
-            for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
     }
 }
 
@@ -318,7 +355,7 @@ cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
     bin_kernel<<<slots, kBlock, 0, s>>>(a);
     scan_kernel<<<a.nboxes, kScanThreads, 0, s>>>(a);
     scatter_kernel<<<slots, kBlock, 0, s>>>(a);
-    sort_kernel<<<blocks_for((uint64_t)a.ncells * 32u), kBlock, 0, s>>>(a);
+    sort_kernel<<<(unsigned)sm_count() * 8u, kBlock, 0, s>>>(a);
     reorder_kernel<<<slots, kBlock, 0, s>>>(a);
     pack_kernel<<<slots, kBlock, 0, s>>>(a);
     launch_build_list(a, s);  // vlj_build.cu

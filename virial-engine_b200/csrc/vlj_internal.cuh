@@ -108,6 +108,8 @@ struct Global {
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
     uint32_t max_count;          // longest list built so far
+    uint32_t work_cells;         // entries of Arena::work this step
+    uint32_t next_build;         // next work entry the list build takes
     uint32_t pad;
 };
 
@@ -138,6 +140,9 @@ struct Arena {
     uint32_t* sorted;
     uint32_t* cell_start;  // ncells + 1
     uint32_t* count;
+    // the non-empty cells of the boxes that rebuild this step, in no set
+    // order (the scan appends them; the sort and the list build take them)
+    uint32_t* work;
     uint32_t* list_count;
     uint32_t* list;
     // per force block (kForceThreads slots): rows (four entries each) of the
