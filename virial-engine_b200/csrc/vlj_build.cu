@@ -13,11 +13,14 @@
 // warp reads the 27 neighbour cells' ranges at once (a lane each), which makes
 // the cells' candidates one stream in stencil order; it fetches the stream
 // kRound candidates at a time (slot, then encoded position, all loads of a
-// round in flight together), copies those within reach of the home cell into
-// shared memory, then every lane tests its home particle against each staged
-// candidate in turn -- the same candidates in the same order for all lanes, so
-// the warp never diverges on the stream and the inner loop reads only shared
-// memory. A dense home cell costs a few rounds of two dependent loads.
+// round in flight together) and copies those within reach of the home cell
+// into shared memory (a dense cell's all of them). A cell of kLaneHomes or
+// more particles then gives each lane a home particle to test against every
+// staged candidate in stream order; a sparser cell (dilute boxes) takes its
+// home particles in turn, the 32 lanes testing 32 staged candidates at once
+// and a ballot placing the accepted ones in the list in stream order. Either
+// way the inner loop reads only shared memory, and a dense home cell costs a
+// few rounds of two dependent loads.
 //
 // A test on the 32-bit encoded positions settles every candidate farther than
 // sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in); the two radii
@@ -31,10 +34,12 @@
 
 namespace vlj {
 
-constexpr int kBuildWarps = 8;  // warps per block, each building one home cell at a time
-constexpr int kRound = 128;     // candidates a warp fetches and stages per round
+constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
+constexpr int kRound = 128;     // candidates a warp fetches per round
+constexpr int kStage = 512;     // staged candidates a warp holds (a dense cell's all)
+constexpr int kLaneHomes = 12;  // home particles from which a lane takes one each
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
-#define VLJ_BUILD_BLOCKS_PER_SM 3
+#define VLJ_BUILD_BLOCKS_PER_SM 6
 #endif
 constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;  // register budget of the build
 
@@ -72,8 +77,9 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     count_kernel(a);
     if (!a.glob->any) return;
     __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
-    __shared__ uint32_t s_j[kBuildWarps][kRound];
-    __shared__ uint4 s_enc[kBuildWarps][kRound];
+    // staged candidates: (x, y, z) as f32 offsets from the home cell's centre
+    // (wide boxes) or as encoded words (narrow ones), the slot in w
+    __shared__ uint4 s_cand[kBuildWarps][kStage];
     for (int t = threadIdx.x; t < 512; t += blockDim.x)
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
     __syncthreads();
@@ -108,7 +114,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                                   (int32_t)(lane / 9u) - 1};
             if (!repeats(d[0], n[0]) && !repeats(d[1], n[1]) && !repeats(d[2], n[2])) {
                 int32_t u[3];
-    #pragma unroll
+#pragma unroll
                 for (int k = 0; k < 3; k++) {
                     u[k] = c[k] + d[k];
                     u[k] = u[k] < 0 ? u[k] + n[k] : (u[k] >= n[k] ? u[k] - n[k] : u[k]);
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
             }
         }
         uint32_t off = cnt;
-    #pragma unroll
+#pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t t = __shfl_up_sync(0xffffffffu, off, o);
             if (lane >= (uint32_t)o) off += t;
@@ -132,54 +138,70 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
         // staging filter: a candidate farther than reach_r2 from the whole home
         // cell cannot be in any home particle's list.
         uint32_t home_lo[3], home_w[3];
-    #pragma unroll
+#pragma unroll
         for (int k = 0; k < 3; k++) {
             home_lo[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)c[k] * (double)bx.cell_size_f[k] * bx.enc[k]);
             home_w[k] = (uint32_t)(unsigned long long)__double2ll_rn((double)bx.cell_size_f[k] * bx.enc[k]);
         }
         const float reach_r2 = bx.reach_r2;
+        // In a box at least five cells wide on every axis, a home particle and
+        // a candidate within reach lie less than 0.3 of a side from the home
+        // cell's centre, so the plain difference of their f32 offsets from it
+        // is the nearest image, within 1e-6 of the exact separation -- far
+        // inside the accept / prefilter margins. Narrower boxes (batched
+        // replicas) test on the encoded words, which wrap to the nearest image.
+        const bool wide = n[0] >= 5 && n[1] >= 5 && n[2] >= 5;
+        uint32_t mid[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) mid[k] = home_lo[k] + home_w[k] / 2u;
         const size_t row_stride = (size_t)a.seg * 4u;
         const unsigned below = (1u << lane) - 1u;
         for (uint32_t h0 = hbeg; h0 < hend; h0 += 32) {
             const bool home = h0 + lane < hend;
             const uint32_t i = home ? a.sorted[h0 + lane] : 0u;
             const uint4 own_enc = home ? cur[i] : make_uint4(0u, 0u, 0u, 0u);
-            uint32_t found = 0;
-            // where the next entry goes: row (found / 4), column (found % 4)
-            uint32_t* wrow = a.list + (size_t)i * 4u;
-            uint32_t wcol = 0;
+            // offsets from the home cell's centre (wide boxes); a lane with no
+            // home particle sits far away and accepts nothing
+            float own_rel[3] = {3.0e18f, 3.0e18f, 3.0e18f};
+            if (home) {
+                own_rel[0] = (float)(int32_t)(own_enc.x - mid[0]) * dec[0];
+                own_rel[1] = (float)(int32_t)(own_enc.y - mid[1]) * dec[1];
+                own_rel[2] = (float)(int32_t)(own_enc.z - mid[2]) * dec[2];
+            }
+            uint32_t found = 0;  // this lane's home particle's list length so far
+            const uint32_t homes = min(hend - h0, 32u);
+            uint32_t staged = 0;
             for (uint32_t base = 0; base < total; base += kRound) {
                 // Fetch the next kRound candidates of the stream (kRound / 32 per
                 // lane, loads in flight together), keep those within reach of the
                 // home cell, and stage them in stream order.
                 uint32_t j[kRound / 32];
-    #pragma unroll
+#pragma unroll
                 for (int r = 0; r < kRound / 32; r++) {
                     const uint32_t t = base + (uint32_t)r * 32u + lane;
                     // the last stencil lane whose stream offset is <= t (all
                     // lanes search, past-the-end ones for the last candidate)
                     const uint32_t tt = t < total ? t : total - 1u;
                     uint32_t lo = 0, hi = 32;
-    #pragma unroll
+#pragma unroll
                     for (int q = 0; q < 5; q++) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (__shfl_sync(0xffffffffu, off, mid) <= tt) lo = mid; else hi = mid;
+                        const uint32_t m = (lo + hi) >> 1;
+                        if (__shfl_sync(0xffffffffu, off, m) <= tt) lo = m; else hi = m;
                     }
                     const uint32_t from = __shfl_sync(0xffffffffu, cs, lo);
                     const uint32_t at = __shfl_sync(0xffffffffu, off, lo);
                     j[r] = t < total ? a.sorted[from + t - at] : 0xffffffffu;
                 }
                 uint4 pe[kRound / 32];
-    #pragma unroll
+#pragma unroll
                 for (int r = 0; r < kRound / 32; r++)
                     pe[r] = j[r] != 0xffffffffu ? __ldg(cur + j[r]) : make_uint4(0u, 0u, 0u, 0u);
-                uint32_t staged = 0;
-    #pragma unroll
+#pragma unroll
                 for (int r = 0; r < kRound / 32; r++) {
                     bool keep = false;
                     if (j[r] != 0xffffffffu) {
                         float g2 = 0.0f;
-    #pragma unroll
+#pragma unroll
                         for (int k = 0; k < 3; k++) {
                             // periodic gap between the candidate and the interval
                             // [lo, lo + w): above it, or below it around the box,
@@ -195,28 +217,83 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                     const unsigned kept_mask = __ballot_sync(0xffffffffu, keep);
                     if (keep) {
                         const uint32_t to = staged + (uint32_t)__popc(kept_mask & below);
-                        s_j[warp][to] = j[r];
-                        s_enc[warp][to] = pe[r];
+                        if (wide)
+                            s_cand[warp][to] = make_uint4(
+                                __float_as_uint((float)(int32_t)(pe[r].x - mid[0]) * dec[0]),
+                                __float_as_uint((float)(int32_t)(pe[r].y - mid[1]) * dec[1]),
+                                __float_as_uint((float)(int32_t)(pe[r].z - mid[2]) * dec[2]), j[r]);
+                        else
+                            s_cand[warp][to] = make_uint4(pe[r].x, pe[r].y, pe[r].z, j[r]);
                     }
                     staged += (uint32_t)__popc(kept_mask);
                 }
+                // test once the stream is done or the stage has no room for
+                // another round
+                if (base + kRound < total && staged + kRound <= (uint32_t)kStage) continue;
                 __syncwarp();
-                for (uint32_t q = 0; q < staged; q++) {
-                    const uint32_t jq = s_j[warp][q];
-                    const float r2e = encoded_r2(s_enc[warp][q], own_enc, dec);
-                    bool in = r2e < acc_r2;
-                    if (!in && r2e < pre_r2 && home && jq != i) in = ref_test(a, bx, i, jq, s_q510);
-                    if (in && home && jq != i) {
-                        if (found < cap) wrow[wcol] = jq;
-                        found += 1;
-                        wcol += 1;
-                        if (wcol == 4u) {
-                            wcol = 0;
-                            wrow += row_stride;
+                // Squared separation of staged candidate e from a home
+                // particle at offsets (ox, oy, oz) / encoded words oe.
+                auto sep2 = [&](const uint4& e, float ox, float oy, float oz, const uint4& oe) {
+                    if (wide) {
+                        const float dx = __uint_as_float(e.x) - ox;
+                        const float dy = __uint_as_float(e.y) - oy;
+                        const float dz = __uint_as_float(e.z) - oz;
+                        return dx * dx + dy * dy + dz * dz;
+                    }
+                    return encoded_r2(e, oe, dec);
+                };
+                if (homes >= (uint32_t)kLaneHomes) {
+                    // Full cells: each lane tests its home particle against
+                    // every staged candidate in stream order (one broadcast
+                    // shared-memory read per candidate for the whole warp).
+                    uint32_t* row_of_i = a.list + (size_t)i * 4u;
+                    for (uint32_t q = 0; q < staged; q++) {
+                        const uint4 e = s_cand[warp][q];
+                        const float r2e = sep2(e, own_rel[0], own_rel[1], own_rel[2], own_enc);
+                        if (home && r2e < pre_r2 && e.w != i &&
+                            (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510))) {
+                            if (found < cap)
+                                row_of_i[(size_t)(found >> 2) * row_stride + (found & 3u)] = e.w;
+                            found += 1;
                         }
+                    }
+                } else {
+                    // Sparse cells: each home particle in turn against 32
+                    // staged candidates at once (a lane each); a ballot puts
+                    // the accepted ones in the list in stream order.
+                    for (uint32_t h = 0; h < homes; h++) {
+                        const uint32_t ih = __shfl_sync(0xffffffffu, i, h);
+                        uint32_t fh = __shfl_sync(0xffffffffu, found, h);
+                        const float ox = __shfl_sync(0xffffffffu, own_rel[0], h);
+                        const float oy = __shfl_sync(0xffffffffu, own_rel[1], h);
+                        const float oz = __shfl_sync(0xffffffffu, own_rel[2], h);
+                        const uint4 oe = make_uint4(__shfl_sync(0xffffffffu, own_enc.x, h),
+                                                    __shfl_sync(0xffffffffu, own_enc.y, h),
+                                                    __shfl_sync(0xffffffffu, own_enc.z, h), 0u);
+                        uint32_t* row_of_ih = a.list + (size_t)ih * 4u;
+                        for (uint32_t q0 = 0; q0 < staged; q0 += 32) {
+                            const uint32_t q = q0 + lane;
+                            bool in = false;
+                            uint32_t jq = 0;
+                            if (q < staged) {
+                                const uint4 e = s_cand[warp][q];
+                                const float r2e = sep2(e, ox, oy, oz, oe);
+                                jq = e.w;
+                                if (r2e < pre_r2 && jq != ih)
+                                    in = r2e < acc_r2 || ref_test(a, bx, ih, jq, s_q510);
+                            }
+                            const unsigned acc = __ballot_sync(0xffffffffu, in);
+                            if (in) {
+                                const uint32_t k = fh + (uint32_t)__popc(acc & below);
+                                if (k < cap) row_of_ih[(size_t)(k >> 2) * row_stride + (k & 3u)] = jq;
+                            }
+                            fh += (uint32_t)__popc(acc);
+                        }
+                        if (lane == h) found = fh;
                     }
                 }
                 __syncwarp();
+                staged = 0;
             }
             const uint32_t kept = found < cap ? found : cap;
             if (home) {
