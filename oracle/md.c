@@ -7,7 +7,8 @@
  * velocity Verlet or BAOAB Langevin (lennard_jones.wgsl:225-276, 556-574)
  * with velocities stored half a kick behind so one force pass serves the
  * closing half kick of one step and the opening half kick of the next, and
- * Langevin noise from the Philox stream keyed by (seed, step, particle id).
+ * Langevin noise from the Philox stream keyed by (seed, step, particle id);
+ * or Nose-Hoover (lennard_jones.wgsl:309-397) on canonical velocities.
  * Everything is f64; particles are kept in cell order (reordered at every
  * rebuild) and the loops run under OpenMP. Test oracle only.
  */
@@ -28,6 +29,8 @@ struct vo_md {
     int shifted_force;
     int thermostat;
     double c1, c2;
+    /* Nose-Hoover: g k T, Q, and the thermostat's xi and eta */
+    double nh_gkt, nh_q, xi, eta;
     uint32_t seed;
     double uc, fc; /* U(rc) and F(rc) for the shifts */
     /* slot-ordered state: positions, velocities half a kick behind, ids */
@@ -203,6 +206,45 @@ static double wrap(double x, double side) {
     return x;
 }
 
+/* One Nose-Hoover half step (lennard_jones.wgsl:309-397, Tuckerman's
+ * time-reversible splitting): xi a quarter step with the kinetic energy,
+ * eta a half step, the velocity scale s = exp(-xi dt / 2), xi another quarter
+ * step with the kinetic energy after scaling, then v <- s v. The velocities
+ * here are the canonical ones. */
+static void nh_half(vo_md *m) {
+    double ke = 0.0;
+#pragma omp parallel for reduction(+ : ke) schedule(static)
+    for (size_t q = 0; q < 3 * (size_t)m->n; q++) ke += 0.5 * m->vm[q] * m->vm[q];
+    double quarter = 0.25 * m->dt, half = 0.5 * m->dt;
+    m->xi += (2.0 * ke - m->nh_gkt) / m->nh_q * quarter;
+    double s = exp(-m->xi * half);
+    m->eta += m->xi * half;
+    double ke2 = ke * s * s;
+    m->xi += (2.0 * ke2 - m->nh_gkt) / m->nh_q * quarter;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < 3 * (size_t)m->n; q++) m->vm[q] *= s;
+}
+
+/* A Nose-Hoover step (lennard_jones.rs:1108-1127): thermostat half step,
+ * half kick, drift, lists, forces, half kick, thermostat half step. */
+static void nh_step(vo_md *m) {
+    nh_half(m);
+    double dt = m->dt, half = 0.5 * m->dt;
+#pragma omp parallel for schedule(static)
+    for (uint32_t i = 0; i < m->n; i++)
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)i + k;
+            m->vm[q] += m->a[q] * half;
+            m->x[q] = wrap(m->x[q] + m->vm[q] * dt, m->box[k]);
+        }
+    m->step += 1;
+    if (needs_rebuild(m)) rebuild(m);
+    forces(m, 0);
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < 3 * (size_t)m->n; q++) m->vm[q] += m->a[q] * half;
+    nh_half(m);
+}
+
 /* Closing half kick of the previous step + opening half kick of this one,
  * then the drift (with friction and noise for Langevin). */
 static void advance(vo_md *m) {
@@ -248,6 +290,13 @@ vo_md *vo_md_create(const double *pos, const double *vel, uint32_t n, const doub
     if (thermostat == 1) {
         m->c1 = exp(-friction * dt);
         m->c2 = sqrt((1.0 - m->c1 * m->c1) * temperature);
+    }
+    if (thermostat == 2) {
+        /* lennard_jones.rs:516-528: g = 3N - 3 (zero total momentum),
+         * Q = g T period^2 / (4 pi^2); `friction` carries the period */
+        double dof = 3.0 * (double)n - 3.0;
+        m->nh_gkt = dof * temperature;
+        m->nh_q = dof * temperature * friction * friction / (4.0 * 3.141592653589793 * 3.141592653589793);
     }
     m->seed = seed;
     double sc6 = 1.0 / (m->rc2 * m->rc2 * m->rc2);
@@ -295,7 +344,8 @@ vo_md *vo_md_create(const double *pos, const double *vel, uint32_t n, const doub
         for (int k = 0; k < 3; k++) m->vm[3 * (size_t)i + k] = vel[3 * (size_t)i + k];
     rebuild(m);
     forces(m, 0);
-    for (size_t q = 0; q < 3 * (size_t)n; q++) m->vm[q] -= m->a[q] * 0.5 * dt;
+    if (thermostat != 2)
+        for (size_t q = 0; q < 3 * (size_t)n; q++) m->vm[q] -= m->a[q] * 0.5 * dt;
     return m;
 }
 
@@ -320,6 +370,10 @@ void vo_md_destroy(vo_md *m) {
 }
 
 void vo_md_run(vo_md *m, uint64_t steps) {
+    if (m->thermostat == 2) {
+        for (uint64_t s = 0; s < steps; s++) nh_step(m);
+        return;
+    }
     for (uint64_t s = 0; s < steps; s++) {
         if (needs_rebuild(m)) rebuild(m);
         forces(m, 0);
@@ -331,7 +385,8 @@ void vo_md_measure(vo_md *m, vo_md_measurement *out) {
     if (needs_rebuild(m)) rebuild(m);
     forces(m, 1);
     double ke = 0.0, pe = 0.0, w = 0.0, p0 = 0.0, p1 = 0.0, p2 = 0.0;
-    double half = 0.5 * m->dt;
+    /* Nose-Hoover keeps canonical velocities; otherwise half a kick behind */
+    double half = m->thermostat == 2 ? 0.0 : 0.5 * m->dt;
     for (uint32_t i = 0; i < m->n; i++) {
         double v[3];
         for (int k = 0; k < 3; k++) v[k] = m->vm[3 * (size_t)i + k] + m->a[3 * (size_t)i + k] * half;
@@ -350,12 +405,14 @@ void vo_md_measure(vo_md *m, vo_md_measurement *out) {
     out->momentum[1] = p1;
     out->momentum[2] = p2;
     out->list_rebuilds = m->rebuilds;
+    out->thermostat_energy =
+        m->thermostat == 2 ? 0.5 * m->nh_q * m->xi * m->xi + m->nh_gkt * m->eta : 0.0;
 }
 
 void vo_md_read(vo_md *m, double *pos, double *vel) {
     if (needs_rebuild(m)) rebuild(m);
     forces(m, 0);
-    double half = 0.5 * m->dt;
+    double half = m->thermostat == 2 ? 0.0 : 0.5 * m->dt;
     for (uint32_t i = 0; i < m->n; i++) {
         uint32_t id = m->ids[i];
         for (int k = 0; k < 3; k++) {

@@ -62,6 +62,7 @@ class MdMeasurement(C.Structure):
         ("virial", C.c_double),
         ("momentum", C.c_double * 3),
         ("list_rebuilds", C.c_uint32),
+        ("thermostat_energy", C.c_double),
     ]
 
 
@@ -276,11 +277,14 @@ class MD:
     """f64 cell-list MD with the CUDA path's integrator (the CPU baseline)."""
 
     def __init__(self, pos, vel, box, cutoff=2.5, skin=0.3, dt=0.005, shifted_force=False,
-                 langevin=None):
+                 langevin=None, nose_hoover=None):
         thermostat, t, gamma, seed = 0, 0.0, 0.0, 0
         if langevin is not None:
             thermostat = 1
             t, gamma, seed = langevin
+        elif nose_hoover is not None:
+            thermostat = 2
+            t, gamma = nose_hoover  # temperature, period
         self._h = _lib.vo_md_create(_f64(pos), _f64(vel), len(pos), _f64(box), cutoff, skin, dt,
                                     int(shifted_force), thermostat, t, gamma, seed)
         self.n = len(pos)

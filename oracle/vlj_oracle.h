@@ -143,9 +143,11 @@ typedef struct {
     uint64_t step;
     double kinetic, potential, virial, momentum[3];
     uint32_t list_rebuilds;
+    double thermostat_energy; /* Nose-Hoover: Q xi^2 / 2 + g k T eta */
 } vo_md_measurement;
 
-/* thermostat: 0 constant energy, 1 Langevin (temperature, friction, seed). */
+/* thermostat: 0 constant energy, 1 Langevin (temperature, friction, seed),
+ * 2 Nose-Hoover (temperature, `friction` read as the period). */
 vo_md *vo_md_create(const double *pos, const double *vel, uint32_t n, const double box[3],
                     double cutoff, double skin, double dt, int shifted_force,
                     int thermostat, double temperature, double friction, uint32_t seed);

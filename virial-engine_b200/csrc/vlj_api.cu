@@ -132,6 +132,14 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
         b.c2 = std::sqrt((1.0 - b.c1 * b.c1) * t.temperature);
         b.seed = t.seed;
     }
+    b.nh_q = 1.0;
+    if (t.kind == VLJ_THERMOSTAT_NOSE_HOOVER) {
+        // lennard_jones.rs:516-528: g = 3N - 3 (zero total momentum),
+        // Q = g T period^2 / (4 pi^2)
+        const double dof = 3.0 * (double)count - 3.0;
+        b.nh_gkt = dof * t.temperature;
+        b.nh_q = dof * t.temperature * t.period * t.period / (4.0 * M_PI * M_PI);
+    }
     b.near_count = 4;
     b.drawn = VLJ_DRAWN_NEIGHBOURS;
     b.reorder_every = 4;
@@ -216,7 +224,13 @@ vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_encode(s->arena, s->stream));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
-    CUDA_TRY(launch_prime(s->arena, s->list_map, s->shifted_force, s->stream));
+    if (s->nose_hoover) {
+        // the thermostat starts at rest (xi = eta = 0) from the given velocities
+        CUDA_TRY(cudaMemsetAsync(s->arena.nh, 0, sizeof(Thermo), s->stream));
+        CUDA_TRY(launch_nh_force(s->arena, s->list_map, s->shifted_force, true, s->stream));
+    } else {
+        CUDA_TRY(launch_prime(s->arena, s->list_map, s->shifted_force, s->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return VLJ_OK;
 }
@@ -244,7 +258,9 @@ vlj_measurement decode(const vlj_sim* s, const Readback& r, uint64_t step) {
     m.list_rebuilds = r.ctrl.rebuilds;
     m.list_overflow = r.ctrl.overflow;
     m.condensed = (uint32_t)std::llround(value(r.slots[6]));
-    m.thermostat_energy = 0.0;
+    // lennard_jones.rs:1235-1241: Q xi^2 / 2 + g k T eta
+    m.thermostat_energy = s->nose_hoover
+        ? 0.5 * s->box.nh_q * r.nh.xi_m * r.nh.xi_m + s->box.nh_gkt * r.nh.eta_m : 0.0;
     return m;
 }
 
@@ -258,6 +274,9 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
                                  s->stream));
         CUDA_TRY(cudaMemcpyAsync(&r->ctrl, s->arena.ctrl, sizeof(Control), cudaMemcpyDeviceToHost,
                                  s->stream));
+        if (s->nose_hoover)
+            CUDA_TRY(cudaMemcpyAsync(&r->nh, s->arena.nh, sizeof(Thermo), cudaMemcpyDeviceToHost,
+                                     s->stream));
         CUDA_TRY(cudaEventRecord(s->ring_event[slot], s->stream));
         s->ring_busy[slot] = true;
         s->ring_step[slot] = s->steps;
@@ -309,13 +328,14 @@ vlj_status vlj_create(const vlj_particle* particles, size_t count, const vlj_set
     int devices = 0;
     vlj_device_count(&devices);
     if (devices == 0) return fail(VLJ_NO_DEVICE, "no CUDA device is visible");
-    if (settings->thermostat.kind == VLJ_THERMOSTAT_NOSE_HOOVER)
-        return fail(VLJ_NOT_ENABLED, "the Nose-Hoover thermostat is not available in this build");
+    if (settings->thermostat.kind == VLJ_THERMOSTAT_NOSE_HOOVER && count < 2)
+        return fail(VLJ_INVALID_ARG, "Nose-Hoover needs at least two particles");
 
     vlj_sim* s = new vlj_sim();
     s->settings = *settings;
     s->n = (uint32_t)count;
     s->shifted_force = settings->shifted_force != 0;
+    s->nose_hoover = settings->thermostat.kind == VLJ_THERMOSTAT_NOSE_HOOVER;
     vlj_status st = make_box(particles, count, settings->box_size, settings->cutoff,
                              settings->skin, settings->dt, s->shifted_force, settings->thermostat,
                              settings->profile_bins, s->box, 3);
@@ -518,6 +538,12 @@ vlj_status vlj_set_temperature(vlj_sim* s, double temperature) {
     if (t.kind == VLJ_THERMOSTAT_LANGEVIN) {
         double c1 = std::exp(-t.friction * s->settings.dt);
         s->box.c2 = std::sqrt((1.0 - c1 * c1) * temperature);
+    } else {
+        if (!(temperature > 0.0))
+            return fail(VLJ_INVALID_ARG, "Nose-Hoover needs a temperature above zero");
+        const double dof = 3.0 * (double)s->n - 3.0;
+        s->box.nh_gkt = dof * temperature;
+        s->box.nh_q = dof * temperature * t.period * t.period / (4.0 * M_PI * M_PI);
     }
     return push_box(s);
 }
@@ -817,6 +843,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.sid, seg));
     TRY(dalloc(s, &a.scell, seg));
     TRY(dalloc(s, &a.accum, (size_t)kSlots * boxes.size()));
+    TRY(dalloc(s, &a.nh, boxes.size()));
+    if (s->nose_hoover) TRY(dalloc(s, &a.acc, seg));
     TRY(dalloc(s, &a.pe_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.w_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.vel4, seg));
@@ -858,8 +886,9 @@ static vlj_status end_capture(cudaStream_t cs, cudaError_t launched, cudaGraphNo
 }
 
 // A graph of `count` steps: decide -> IF(some box rebuilds){rebuild chain} ->
-// step kernel, chained. The decide kernel sets the condition on the device,
-// so a step with no rebuild launches no rebuild kernel at all.
+// step kernel, chained (Nose-Hoover: nh_begin -> decide -> IF{...} ->
+// nh_force). The decide kernel sets the condition on the device, so a step
+// with no rebuild launches no rebuild kernel at all.
 static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaGraphCreate(&g, 0));
@@ -876,7 +905,10 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         cudaGraphNode_t n_decide = nullptr, n_cond = nullptr;
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, prev ? &prev : nullptr, nullptr, prev ? 1 : 0,
                                                mode));
-        TRY(end_capture(cs, launch_decide(s->arena, cs, h), &n_decide));
+        cudaError_t e = cudaSuccess;
+        if (s->nose_hoover) e = launch_nh_begin(s->arena, cs);
+        if (e == cudaSuccess) e = launch_decide(s->arena, cs, h);
+        TRY(end_capture(cs, e, &n_decide));
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.conditional.handle = h;
         cp.conditional.type = cudaGraphCondTypeIf;
@@ -886,13 +918,24 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
         TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
-        TRY(end_capture(cs, launch_step(s->arena, s->list_map, s->shifted_force, cs), &prev));
+        TRY(end_capture(cs,
+                        s->nose_hoover
+                            ? launch_nh_force(s->arena, s->list_map, s->shifted_force, false, cs)
+                            : launch_step(s->arena, s->list_map, s->shifted_force, cs),
+                        &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
     return VLJ_OK;
 }
 
 static vlj_status step_direct(vlj_sim* s) {
+    if (s->nose_hoover) {
+        CUDA_TRY(launch_nh_begin(s->arena, s->stream));
+        CUDA_TRY(launch_decide(s->arena, s->stream, 0));
+        CUDA_TRY(launch_rebuild(s->arena, s->stream));
+        CUDA_TRY(launch_nh_force(s->arena, s->list_map, s->shifted_force, false, s->stream));
+        return VLJ_OK;
+    }
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
     if (s->timing) {

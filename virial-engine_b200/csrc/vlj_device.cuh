@@ -111,6 +111,30 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+// One Nose-Hoover half step of (xi, eta) (lennard_jones.wgsl:341-377): xi a
+// quarter step with the kinetic energy ke, the velocity scale
+// s = exp(-xi dt / 2), eta a half step, xi another quarter step with the
+// kinetic energy after scaling. Returns s; ke becomes ke s^2.
+__device__ __forceinline__ double nh_half(const Box& bx, double& xi, double& eta, double& ke) {
+    const double quarter = 0.5 * bx.half_dt;
+    xi += (2.0 * ke - bx.nh_gkt) / bx.nh_q * quarter;
+    const double s = exp(-xi * bx.half_dt);
+    eta += xi * bx.half_dt;
+    ke = ke * s * s;
+    xi += (2.0 * ke - bx.nh_gkt) / bx.nh_q * quarter;
+    return s;
+}
+
+// Canonical velocity component k of slot i: the stored one plus the closing
+// half kick (velocities half a kick behind), or for Nose-Hoover the stored
+// one times the end half step's pending scale.
+__device__ __forceinline__ double canonical_velocity(const Arena& a, const Box& bx, uint32_t b,
+                                                     uint32_t i, int k, float acc) {
+    const double v = a.v[(size_t)k * a.seg + i];
+    if (bx.thermostat == 2) return v * a.nh[b].scale;
+    return v + (double)acc * bx.half_dt;
+}
+
 // Periodic wrap of an f64 coordinate that moved less than one side.
 __device__ __forceinline__ double wrap(double x, double side) {
     if (x >= side) x -= side;

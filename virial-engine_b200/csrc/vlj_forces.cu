@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kForceThreads) measure_kernel(Arena a,
         double vel[3], ke = 0.0;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            vel[k] = a.v[(size_t)k * a.seg + i] + (double)acc[k] * bx.half_dt;
+            vel[k] = canonical_velocity(a, bx, b, i, k, acc[k]);
             ke += vel[k] * vel[k];
             if (canonical) a.vcanon[(size_t)k * a.seg + i] = vel[k];
         }
@@ -332,6 +332,121 @@ __global__ void __launch_bounds__(kForceThreads) measure_kernel(Arena a,
         a.vel4[i] = make_float4((float)vel[0], (float)vel[1], (float)vel[2], (float)s.near);
     }
     block_sum_slots(a, valid, b, blockIdx.x * kForceThreads, v);
+}
+
+// ---- Nose-Hoover (lennard_jones.wgsl:309-397; host lennard_jones.rs:1108-1127) ----
+// One box. A step runs nh_begin (the pending end-half scale s2 of the last
+// step and this step's start-half scale s1, the half kick, the drift), the
+// decision and rebuild, then nh_force (forces, the closing half kick, the
+// kinetic energy, and the end half step's xi / eta update in the block that
+// finishes last). The stored velocity is the canonical one before s2.
+
+// nh_begin: every thread takes the start half step from the same state, so
+// all of them compute the same s1; the box's first thread stores the result.
+__global__ void __launch_bounds__(kBlock) nh_begin_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < a.nslots;
+    const uint32_t phase = a.glob->phase;
+    const uint32_t b = valid ? box_of_slot(a, i) : 0u;
+    const Box& bx = a.boxes[b];
+    float disp2 = 0.0f;
+    if (valid) {
+        const Thermo& t = a.nh[b];
+        double xi = t.xi_m, eta = t.eta_m, ke = t.ke_m;
+        const double s2 = t.scale;
+        const double s1 = nh_half(bx, xi, eta, ke);
+        if (i == bx.first) {
+            a.nh[b].xi_s = xi;
+            a.nh[b].eta_s = eta;
+        }
+        const float4 f = a.acc[i];
+        const float acc[3] = {f.x, f.y, f.z};
+        const uint4 snap = a.snap[i];
+        const uint32_t sw[3] = {snap.x, snap.y, snap.z};
+        uint32_t enc[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t q = (size_t)k * a.seg + i;
+            const double v = a.v[q] * s2 * s1 + (double)acc[k] * bx.half_dt;
+            const double x = wrap(a.x[q] + v * bx.dt, bx.box[k]);
+            a.x[q] = x;
+            a.v[q] = v;
+            enc[k] = encode(x, bx.enc[k]);
+            const float d = decode_diff(enc[k], sw[k], bx.dec[k]);
+            disp2 += d * d;
+        }
+        a.cache[phase ^ 1u][i] = make_uint4(enc[0], enc[1], enc[2], 0u);
+    }
+    block_max_per_box(a, valid, b, blockIdx.x * blockDim.x, disp2);
+    if (i == 0) a.glob->pending = 1u;
+}
+
+// nh_force: forces from the list, the closing half kick (not with PRIME,
+// which only records the first forces), and the kinetic energy summed exactly
+// in 32.32 fixed point; the last block to add its part does the end half
+// step's thermostat update (with PRIME: records the starting kinetic energy).
+template <bool SHIFTED_FORCE, bool PRIME>
+__global__ void __launch_bounds__(kForceThreads) nh_force_kernel(Arena a,
+                                                                 const __grid_constant__ CUtensorMap map) {
+    count_kernel(a);
+    __shared__ __align__(128) Stage st;
+    __shared__ long long s_ke[kForceThreads / 32];
+    __shared__ int s_last;
+    const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
+    const bool valid = i < a.nslots;
+    const Box& bx = a.boxes[0];
+    const PairSums s =
+        block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, valid, a.cache[a.glob->phase]);
+    long long raw = 0;
+    if (valid) {
+        const float acc[3] = {s.ax, s.ay, s.az};
+        a.acc[i] = make_float4(s.ax, s.ay, s.az, 0.0f);
+        double ke = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t q = (size_t)k * a.seg + i;
+            double v = a.v[q];
+            if (!PRIME) {
+                v += (double)acc[k] * bx.half_dt;
+                a.v[q] = v;
+            }
+            ke += v * v;
+        }
+        raw = fixed_raw_f64(0.5 * ke * (double)bx.energy_scale);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) raw += __shfl_xor_sync(0xffffffffu, raw, o);
+    if (lane == 0) s_ke[warp] = raw;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long sum = 0;
+        for (int w = 0; w < kForceThreads / 32; w++) sum += s_ke[w];
+        Thermo* t = a.nh;
+        if (sum) atomicAdd(&t->ke_raw, (unsigned long long)sum);
+        __threadfence();
+        s_last = atomicAdd(&t->blocks_done, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    // every other block's kinetic energy is in: the thermostat update
+    __threadfence();
+    Thermo* t = a.nh;
+    const long long total = (long long)atomicExch(&t->ke_raw, 0ull);
+    t->blocks_done = 0u;
+    double ke = (double)total / 4294967296.0 / (double)bx.energy_scale;
+    if (PRIME) {
+        t->ke_m = ke;
+        t->scale = 1.0;
+        return;
+    }
+    double xi = t->xi_s, eta = t->eta_s;
+    const double s2 = nh_half(bx, xi, eta, ke);
+    t->xi_m = xi;
+    t->eta_m = eta;
+    t->ke_m = ke;
+    t->scale = s2;
 }
 
 // ---- FP32 calibration: eight independent FMA chains per thread, so the
@@ -380,6 +495,28 @@ cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_
         measure_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, canonical ? 1 : 0);
     else
         measure_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, canonical ? 1 : 0);
+    return after_launch();
+}
+
+cudaError_t launch_nh_begin(const Arena& a, cudaStream_t s) {
+    nh_begin_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_nh_force(const Arena& a, const CUtensorMap& map, bool shifted_force, bool prime,
+                            cudaStream_t s) {
+    const unsigned blocks = particle_blocks(a);
+    if (shifted_force) {
+        if (prime)
+            nh_force_kernel<true, true><<<blocks, kForceThreads, 0, s>>>(a, map);
+        else
+            nh_force_kernel<true, false><<<blocks, kForceThreads, 0, s>>>(a, map);
+    } else {
+        if (prime)
+            nh_force_kernel<false, true><<<blocks, kForceThreads, 0, s>>>(a, map);
+        else
+            nh_force_kernel<false, false><<<blocks, kForceThreads, 0, s>>>(a, map);
+    }
     return after_launch();
 }
 

@@ -61,6 +61,7 @@ struct Box {
     double enc[3];       // 2^32 / side
     double dt, half_dt;
     double c1, c2;       // Langevin v <- c1 v + c2 xi (lennard_jones.rs:520-523)
+    double nh_gkt, nh_q; // Nose-Hoover g k T and Q (lennard_jones.rs:516-528)
     float dec[3];        // side / 2^32, exact in f32
     float box_f[3];
     float cell_size_f[3];
@@ -113,6 +114,23 @@ struct Global {
     uint32_t pad;
 };
 
+// Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).
+// A step is: start half step (scale by s1), half kick, drift, lists, forces,
+// half kick, end half step (scale by s2). The force kernel does the end half
+// step's thermostat update once every block has added its kinetic energy
+// (the last block to finish), but leaves the scaling pending: the velocities
+// stay unscaled, `scale` holds s2, and whatever reads velocities at the step
+// boundary (the measurement, the next step's start) applies it.
+struct Thermo {
+    double xi_s, eta_s;  // after the last start half step
+    double xi_m, eta_m;  // after the last end half step (what a measurement sees)
+    double ke_m;         // kinetic energy after the end half step's scaling
+    double scale;        // s2: the end half step's scale, not yet applied
+    unsigned long long ke_raw;  // this force pass's kinetic energy, 32.32 x energy scale
+    uint32_t blocks_done;       // force blocks that added their part
+    uint32_t pad;
+};
+
 // Fault codes in Global::fault (the first one recorded wins).
 constexpr uint32_t kFaultTmaTimeout = 1;  // a TMA tile never arrived
 
@@ -155,6 +173,9 @@ struct Arena {
     double* sv;
     uint32_t* sid;
     uint32_t* scell;
+    // Nose-Hoover (null without): per-box state, and the last forces
+    Thermo* nh;
+    float4* acc;
     // measurements
     unsigned long long* accum;  // nboxes * kSlots
     float* pe_half;  // (hi, lo) per slot
@@ -311,6 +332,13 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifte
                         cudaStream_t s);
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                            bool canonical, cudaStream_t s);
+// Nose-Hoover steps (one box): nh_begin scales (pending s2 and this step's
+// s1), kicks and drifts; nh_force computes the forces, kicks, and does the end
+// half step's thermostat update. With `prime` nh_force only computes the first
+// forces and the starting kinetic energy.
+cudaError_t launch_nh_begin(const Arena& a, cudaStream_t s);
+cudaError_t launch_nh_force(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
+                            bool prime, cudaStream_t s);
 // Sampling kernels (vlj_sampling.cu): one profile sample added into
 // a.profile, one heat-current sample into a.series slot 1 + 3 * sample.
 cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cudaStream_t s);

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in
         add((uint32_t)home * kProfileSlots, 1ll << 32);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const double v = a.v[(size_t)c * a.seg + i] + (double)acc3[c] * bx.half_dt;
+            const double v = canonical_velocity(a, bx, 0, i, c, acc3[c]);
             add((uint32_t)home * kProfileSlots + 1 + c, fixed_raw_f64(v * v));
             add(bins * kProfileSlots + c, fixed_raw_f32(tot[c]));
         }
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kSampleThreads) heat_current_kernel(Arena a, u
         const float acc3[3] = {ax, ay, az};
         double v[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) v[c] = a.v[(size_t)c * a.seg + i] + (double)acc3[c] * bx.half_dt;
+        for (int c = 0; c < 3; c++) v[c] = canonical_velocity(a, bx, 0, i, c, acc3[c]);
         const double e = 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + (double)epair;
         const double tv[3] = {t[0] * v[0] + t[3] * v[1] + t[4] * v[2],
                               t[3] * v[0] + t[1] * v[1] + t[5] * v[2],

@@ -19,6 +19,7 @@ constexpr uint32_t kGraphChunk = 16;  // steps per graph launch
 struct Readback {
     long long slots[kSlots];
     Control ctrl;
+    Thermo nh;
 };
 
 double scale_for(double magnitude);
@@ -36,6 +37,7 @@ struct vlj_sim {
     vlj_settings settings{};
     uint32_t n = 0;
     bool shifted_force = false;
+    bool nose_hoover = false;  // steps run nh_begin / decide / rebuild / nh_force
     vlj::Box box{};
     // batched: one Box per replica, in slot order (empty for a single box)
     std::vector<vlj::Box> replicas;
