@@ -31,6 +31,11 @@ struct vo_md {
     double c1, c2;
     /* Nose-Hoover: g k T, Q, and the thermostat's xi and eta */
     double nh_gkt, nh_q, xi, eta;
+    /* heat exchange: on, slab bounds (hot lo, hi, cold lo, hi; f32 values),
+     * energy per step (its f32 value) */
+    int hex;
+    float hex_slabs[4];
+    double hex_energy;
     uint32_t seed;
     double uc, fc; /* U(rc) and F(rc) for the shifts */
     /* slot-ordered state: positions, velocities half a kick behind, ids */
@@ -245,6 +250,98 @@ static void nh_step(vo_md *m) {
     nh_half(m);
 }
 
+/* ---- heat exchange, eHEX/a (lennard_jones.wgsl:732-893; Wirnsberger,
+ * Frenkel and Dellago 2015, eq. 20) on canonical velocities ---- */
+static int hex_slab(const vo_md *m, double z) {
+    float zf = (float)z;
+    if (zf >= m->hex_slabs[0] && zf < m->hex_slabs[1]) return 0;
+    if (zf >= m->hex_slabs[2] && zf < m->hex_slabs[3]) return 1;
+    return 2;
+}
+
+static void hex_apply(vo_md *m) {
+    double dt = m->dt, dt3 = dt * dt * dt;
+    double cnt[2] = {0, 0}, p[2][3] = {{0}}, f[2][3] = {{0}}, v2[2] = {0, 0}, fv[2] = {0, 0};
+    for (uint32_t i = 0; i < m->n; i++) {
+        int sl = hex_slab(m, m->x[3 * (size_t)i + 2]);
+        if (sl == 2) continue;
+        const double *v = m->vm + 3 * (size_t)i, *a = m->a + 3 * (size_t)i;
+        cnt[sl] += 1.0;
+        for (int k = 0; k < 3; k++) {
+            p[sl][k] += v[k];
+            f[sl][k] += a[k];
+        }
+        v2[sl] += v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        fv[sl] += a[0] * v[0] + a[1] * v[1] + a[2] * v[2];
+    }
+    double com[2][3] = {{0}}, mf[2][3] = {{0}}, sm1[2] = {0, 0}, cv[2] = {0, 0}, cf[2] = {0, 0};
+    for (int sl = 0; sl < 2; sl++) {
+        double mm = cnt[sl];
+        if (!(mm > 0.0)) continue;
+        for (int k = 0; k < 3; k++) {
+            com[sl][k] = p[sl][k] / mm;
+            mf[sl][k] = f[sl][k] / mm;
+        }
+        double pp = p[sl][0] * p[sl][0] + p[sl][1] * p[sl][1] + p[sl][2] * p[sl][2];
+        double kinetic = 0.5 * v2[sl] - 0.5 * pp / mm;
+        double energy = (sl == 0 ? 1.0 : -1.0) * m->hex_energy;
+        double flux = energy / dt;
+        double x = energy / kinetic;
+        sm1[sl] = x / (1.0 + sqrt(1.0 + x));
+        double power = fv[sl] - (f[sl][0] * com[sl][0] + f[sl][1] * com[sl][1] + f[sl][2] * com[sl][2]);
+        cv[sl] = dt3 * flux / (2.0 * kinetic * kinetic) * (flux / 48.0 + power / 6.0);
+        cf[sl] = dt3 * flux / (12.0 * kinetic);
+    }
+    for (uint32_t i = 0; i < m->n; i++) {
+        int sl = hex_slab(m, m->x[3 * (size_t)i + 2]);
+        if (sl == 2) continue;
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)i + k;
+            double rel = m->vm[q] - com[sl][k];
+            double shift = cv[sl] * rel - cf[sl] * (m->a[q] - mf[sl][k]);
+            m->x[q] = wrap(m->x[q] - shift, m->box[k]);
+            m->vm[q] += sm1[sl] * rel;
+        }
+    }
+}
+
+/* A constant-energy step with the exchange: half kick, drift, lists,
+ * forces, half kick, exchange (lennard_jones.rs:1108-1138). */
+static void hex_step(vo_md *m) {
+    double dt = m->dt, half = 0.5 * m->dt;
+#pragma omp parallel for schedule(static)
+    for (uint32_t i = 0; i < m->n; i++)
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)i + k;
+            m->vm[q] += m->a[q] * half;
+            m->x[q] = wrap(m->x[q] + m->vm[q] * dt, m->box[k]);
+        }
+    m->step += 1;
+    if (needs_rebuild(m)) rebuild(m);
+    forces(m, 0);
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < 3 * (size_t)m->n; q++) m->vm[q] += m->a[q] * half;
+    hex_apply(m);
+}
+
+/* Starts (energy and slabs) or, with on = 0, stops the exchange at the
+ * current step boundary: velocities switch between half a kick behind and
+ * canonical with the forces at the current positions. */
+void vo_md_set_heat_exchange(vo_md *m, int on, const double slabs[4], double energy) {
+    if (on && !m->hex) {
+        if (needs_rebuild(m)) rebuild(m);
+        forces(m, 0);
+        for (size_t q = 0; q < 3 * (size_t)m->n; q++) m->vm[q] += m->a[q] * 0.5 * m->dt;
+    } else if (!on && m->hex) {
+        for (size_t q = 0; q < 3 * (size_t)m->n; q++) m->vm[q] -= m->a[q] * 0.5 * m->dt;
+    }
+    m->hex = on;
+    if (on) {
+        for (int k = 0; k < 4; k++) m->hex_slabs[k] = (float)slabs[k];
+        m->hex_energy = (double)(float)energy;
+    }
+}
+
 /* Closing half kick of the previous step + opening half kick of this one,
  * then the drift (with friction and noise for Langevin). */
 static void advance(vo_md *m) {
@@ -374,6 +471,10 @@ void vo_md_run(vo_md *m, uint64_t steps) {
         for (uint64_t s = 0; s < steps; s++) nh_step(m);
         return;
     }
+    if (m->hex) {
+        for (uint64_t s = 0; s < steps; s++) hex_step(m);
+        return;
+    }
     for (uint64_t s = 0; s < steps; s++) {
         if (needs_rebuild(m)) rebuild(m);
         forces(m, 0);
@@ -385,8 +486,9 @@ void vo_md_measure(vo_md *m, vo_md_measurement *out) {
     if (needs_rebuild(m)) rebuild(m);
     forces(m, 1);
     double ke = 0.0, pe = 0.0, w = 0.0, p0 = 0.0, p1 = 0.0, p2 = 0.0;
-    /* Nose-Hoover keeps canonical velocities; otherwise half a kick behind */
-    double half = m->thermostat == 2 ? 0.0 : 0.5 * m->dt;
+    /* Nose-Hoover and the exchange keep canonical velocities; otherwise half
+     * a kick behind */
+    double half = (m->thermostat == 2 || m->hex) ? 0.0 : 0.5 * m->dt;
     for (uint32_t i = 0; i < m->n; i++) {
         double v[3];
         for (int k = 0; k < 3; k++) v[k] = m->vm[3 * (size_t)i + k] + m->a[3 * (size_t)i + k] * half;
@@ -412,7 +514,7 @@ void vo_md_measure(vo_md *m, vo_md_measurement *out) {
 void vo_md_read(vo_md *m, double *pos, double *vel) {
     if (needs_rebuild(m)) rebuild(m);
     forces(m, 0);
-    double half = m->thermostat == 2 ? 0.0 : 0.5 * m->dt;
+    double half = (m->thermostat == 2 || m->hex) ? 0.0 : 0.5 * m->dt;
     for (uint32_t i = 0; i < m->n; i++) {
         uint32_t id = m->ids[i];
         for (int k = 0; k < 3; k++) {

@@ -109,6 +109,7 @@ _sig("vo_md_destroy", None, [C.c_void_p])
 _sig("vo_md_run", None, [C.c_void_p, C.c_uint64])
 _sig("vo_md_measure", None, [C.c_void_p, C.POINTER(MdMeasurement)])
 _sig("vo_md_read", None, [C.c_void_p, _dp, _dp])
+_sig("vo_md_set_heat_exchange", None, [C.c_void_p, C.c_int, _dp, C.c_double])
 _sig("vo_md_set_threads", None, [C.c_int])
 _sig("vo_md_threads", C.c_int, [])
 
@@ -296,6 +297,12 @@ class MD:
         m = MdMeasurement()
         _lib.vo_md_measure(self._h, C.byref(m))
         return m
+
+    def set_heat_exchange(self, hot=None, cold=None, energy=0.0):
+        """hot and cold (lo, hi) slabs in z, energy per step; None stops."""
+        on = hot is not None
+        slabs = np.array(list(hot) + list(cold) if on else [0.0] * 4, dtype=np.float64)
+        _lib.vo_md_set_heat_exchange(self._h, int(on), slabs, float(energy))
 
     def read(self):
         pos = np.zeros((self.n, 3))

@@ -156,6 +156,9 @@ void vo_md_run(vo_md *md, uint64_t steps);
 void vo_md_measure(vo_md *md, vo_md_measurement *out);
 /* Canonical positions and velocities in input order. */
 void vo_md_read(vo_md *md, double *pos, double *vel);
+/* Heat exchange (eHEX/a) from the next step on: slabs = hot lo, hi, cold lo,
+ * hi in z; energy moved per step; on = 0 stops it. Constant energy only. */
+void vo_md_set_heat_exchange(vo_md *md, int on, const double slabs[4], double energy);
 void vo_md_set_threads(int threads);
 int vo_md_threads(void);
 

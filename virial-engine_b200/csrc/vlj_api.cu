@@ -133,6 +133,7 @@ vlj_status make_box(const vlj_particle* p, size_t count, const double box_size[3
         b.seed = t.seed;
     }
     b.nh_q = 1.0;
+    b.canonical = t.kind == VLJ_THERMOSTAT_NOSE_HOOVER ? 1u : 0u;
     if (t.kind == VLJ_THERMOSTAT_NOSE_HOOVER) {
         // lennard_jones.rs:516-528: g = 3N - 3 (zero total momentum),
         // Q = g T period^2 / (4 pi^2)
@@ -224,10 +225,12 @@ vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_encode(s->arena, s->stream));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
-    if (s->nose_hoover) {
-        // the thermostat starts at rest (xi = eta = 0) from the given velocities
+    if (s->canonical()) {
+        // the thermostat starts at rest (xi = eta = 0) from the given
+        // velocities; the first forces are recorded for the first half kick
         CUDA_TRY(cudaMemsetAsync(s->arena.nh, 0, sizeof(Thermo), s->stream));
-        CUDA_TRY(launch_nh_force(s->arena, s->list_map, s->shifted_force, true, s->stream));
+        CUDA_TRY(cudaMemsetAsync(s->arena.hex, 0, sizeof(Exchange), s->stream));
+        CUDA_TRY(launch_canon_force(s->arena, s->list_map, s->shifted_force, kPrime, s->stream));
     } else {
         CUDA_TRY(launch_prime(s->arena, s->list_map, s->shifted_force, s->stream));
     }
@@ -548,18 +551,57 @@ vlj_status vlj_set_temperature(vlj_sim* s, double temperature) {
     return push_box(s);
 }
 
+// lennard_jones.rs:927-946. Switching the exchange on moves the velocities
+// from half a kick behind to canonical (forces at the current positions);
+// switching it off moves them back. Either way the captured steps change.
 vlj_status vlj_set_heat_exchange(vlj_sim* s, const vlj_heat_exchange* exchange) {
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
     if (s->settings.thermostat.kind != VLJ_THERMOSTAT_NONE)
         return fail(VLJ_NOT_ENABLED, "heat exchange runs at constant energy, without a thermostat");
-    (void)exchange;
-    return fail(VLJ_NOT_ENABLED, "heat exchange is not available in this build");
+    if (exchange) {
+        for (int k = 0; k < 2; k++)
+            if (!std::isfinite(exchange->hot[k]) || !std::isfinite(exchange->cold[k]))
+                return fail(VLJ_INVALID_ARG, "slab bounds must be finite");
+        if (!std::isfinite(exchange->energy))
+            return fail(VLJ_INVALID_ARG, "energy must be finite");
+    }
+    const bool on = exchange != nullptr;
+    if (on != s->exchange) {
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
+        if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
+        s->graph_chunk = s->graph_one = nullptr;
+    }
+    if (on) {
+        s->box.hex_slabs[0] = (float)exchange->hot[0];
+        s->box.hex_slabs[1] = (float)exchange->hot[1];
+        s->box.hex_slabs[2] = (float)exchange->cold[0];
+        s->box.hex_slabs[3] = (float)exchange->cold[1];
+        s->box.hex_energy = (double)(float)exchange->energy;
+        s->exchange_settings = *exchange;
+    }
+    if (on && !s->exchange) {
+        // to canonical velocities: forces now, then the closing half kick
+        TRY(lists_now(s));
+        CUDA_TRY(cudaMemsetAsync(s->arena.hex, 0, sizeof(Exchange), s->stream));
+        CUDA_TRY(launch_canon_force(s->arena, s->list_map, s->shifted_force, kKick, s->stream));
+        s->box.canonical = 1u;
+    } else if (!on && s->exchange) {
+        CUDA_TRY(launch_half_kick_back(s->arena, s->stream));
+        s->box.canonical = 0u;
+        for (int k = 0; k < 4; k++) s->box.hex_slabs[k] = 0.0f;
+        s->box.hex_energy = 0.0;
+    }
+    s->exchange = on;
+    return push_box(s);
 }
 
+// lennard_jones.rs:948-952: the energy moved per step (its f32 value) over 2 A dt.
 vlj_status vlj_heat_flux(const vlj_sim* s, int* has, double* flux) {
     if (!s || !has || !flux) return fail(VLJ_INVALID_ARG, "null argument");
-    *has = 0;
-    *flux = 0.0;
+    *has = s->exchange ? 1 : 0;
+    *flux = s->exchange ? s->box.hex_energy / (2.0 * s->box.box[0] * s->box.box[1] * s->settings.dt)
+                        : 0.0;
     return VLJ_OK;
 }
 
@@ -844,7 +886,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.scell, seg));
     TRY(dalloc(s, &a.accum, (size_t)kSlots * boxes.size()));
     TRY(dalloc(s, &a.nh, boxes.size()));
-    if (s->nose_hoover) TRY(dalloc(s, &a.acc, seg));
+    TRY(dalloc(s, &a.hex, 1));
+    TRY(dalloc(s, &a.acc, seg));
     TRY(dalloc(s, &a.pe_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.w_half, 2 * (size_t)seg));
     TRY(dalloc(s, &a.vel4, seg));
@@ -885,9 +928,19 @@ static vlj_status end_capture(cudaStream_t cs, cudaError_t launched, cudaGraphNo
     return VLJ_OK;
 }
 
+// What follows the rebuild in a step: the fused step kernel, or on canonical
+// velocities the force pass (and the exchange's apply pass).
+static cudaError_t launch_step_tail(vlj_sim* s, cudaStream_t cs) {
+    if (!s->canonical()) return launch_step(s->arena, s->list_map, s->shifted_force, cs);
+    cudaError_t e = launch_canon_force(s->arena, s->list_map, s->shifted_force,
+                                       s->nose_hoover ? kNoseHoover : kExchange, cs);
+    if (e == cudaSuccess && s->exchange) e = launch_hex_apply(s->arena, cs);
+    return e;
+}
+
 // A graph of `count` steps: decide -> IF(some box rebuilds){rebuild chain} ->
-// step kernel, chained (Nose-Hoover: nh_begin -> decide -> IF{...} ->
-// nh_force). The decide kernel sets the condition on the device, so a step
+// step kernel, chained (canonical velocities: begin -> decide -> IF{...} ->
+// canon_force [-> hex_apply]). The decide kernel sets the condition on the device, so a step
 // with no rebuild launches no rebuild kernel at all.
 static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
@@ -906,7 +959,7 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, prev ? &prev : nullptr, nullptr, prev ? 1 : 0,
                                                mode));
         cudaError_t e = cudaSuccess;
-        if (s->nose_hoover) e = launch_nh_begin(s->arena, cs);
+        if (s->canonical()) e = launch_begin(s->arena, cs);
         if (e == cudaSuccess) e = launch_decide(s->arena, cs, h);
         TRY(end_capture(cs, e, &n_decide));
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
@@ -918,22 +971,18 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
         TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
-        TRY(end_capture(cs,
-                        s->nose_hoover
-                            ? launch_nh_force(s->arena, s->list_map, s->shifted_force, false, cs)
-                            : launch_step(s->arena, s->list_map, s->shifted_force, cs),
-                        &prev));
+        TRY(end_capture(cs, launch_step_tail(s, cs), &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
     return VLJ_OK;
 }
 
 static vlj_status step_direct(vlj_sim* s) {
-    if (s->nose_hoover) {
-        CUDA_TRY(launch_nh_begin(s->arena, s->stream));
+    if (s->canonical()) {
+        CUDA_TRY(launch_begin(s->arena, s->stream));
         CUDA_TRY(launch_decide(s->arena, s->stream, 0));
         CUDA_TRY(launch_rebuild(s->arena, s->stream));
-        CUDA_TRY(launch_nh_force(s->arena, s->list_map, s->shifted_force, false, s->stream));
+        CUDA_TRY(launch_step_tail(s, s->stream));
         return VLJ_OK;
     }
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));

@@ -126,12 +126,12 @@ __device__ __forceinline__ double nh_half(const Box& bx, double& xi, double& eta
 }
 
 // Canonical velocity component k of slot i: the stored one plus the closing
-// half kick (velocities half a kick behind), or for Nose-Hoover the stored
-// one times the end half step's pending scale.
+// half kick (velocities half a kick behind), or the stored one itself when the
+// box keeps canonical velocities -- times Nose-Hoover's pending end-half scale.
 __device__ __forceinline__ double canonical_velocity(const Arena& a, const Box& bx, uint32_t b,
                                                      uint32_t i, int k, float acc) {
     const double v = a.v[(size_t)k * a.seg + i];
-    if (bx.thermostat == 2) return v * a.nh[b].scale;
+    if (bx.canonical) return bx.thermostat == 2 ? v * a.nh[b].scale : v;
     return v + (double)acc * bx.half_dt;
 }
 

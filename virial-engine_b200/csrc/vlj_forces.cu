@@ -334,16 +334,20 @@ __global__ void __launch_bounds__(kForceThreads) measure_kernel(Arena a,
     block_sum_slots(a, valid, b, blockIdx.x * kForceThreads, v);
 }
 
-// ---- Nose-Hoover (lennard_jones.wgsl:309-397; host lennard_jones.rs:1108-1127) ----
-// One box. A step runs nh_begin (the pending end-half scale s2 of the last
-// step and this step's start-half scale s1, the half kick, the drift), the
-// decision and rebuild, then nh_force (forces, the closing half kick, the
-// kinetic energy, and the end half step's xi / eta update in the block that
-// finishes last). The stored velocity is the canonical one before s2.
+// ---- steps on canonical velocities: Nose-Hoover (lennard_jones.wgsl:309-397)
+// and the heat exchange (lennard_jones.wgsl:732-893); host order
+// lennard_jones.rs:1108-1138 ----
+// One box. A step runs begin (Nose-Hoover's pending end-half scale s2 of the
+// last step and this step's start-half scale s1, the half kick, the drift),
+// the decision and rebuild, then canon_force (forces, the closing half kick,
+// and the end-of-step sums: the kinetic energy for Nose-Hoover, the slab sums
+// for the exchange; the block that finishes last turns them into the
+// thermostat update or the exchange coefficients), then for the exchange
+// hex_apply. The stored velocity is canonical (before Nose-Hoover's s2).
 
-// nh_begin: every thread takes the start half step from the same state, so
-// all of them compute the same s1; the box's first thread stores the result.
-__global__ void __launch_bounds__(kBlock) nh_begin_kernel(Arena a) {
+// begin: every thread takes the start half step from the same state, so all
+// of them compute the same s1; the box's first thread stores the result.
+__global__ void __launch_bounds__(kBlock) begin_kernel(Arena a) {
     count_kernel(a);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < a.nslots;
@@ -352,13 +356,16 @@ __global__ void __launch_bounds__(kBlock) nh_begin_kernel(Arena a) {
     const Box& bx = a.boxes[b];
     float disp2 = 0.0f;
     if (valid) {
-        const Thermo& t = a.nh[b];
-        double xi = t.xi_m, eta = t.eta_m, ke = t.ke_m;
-        const double s2 = t.scale;
-        const double s1 = nh_half(bx, xi, eta, ke);
-        if (i == bx.first) {
-            a.nh[b].xi_s = xi;
-            a.nh[b].eta_s = eta;
+        double s2 = 1.0, s1 = 1.0;  // exact no-ops without Nose-Hoover
+        if (bx.thermostat == 2) {
+            const Thermo& t = a.nh[b];
+            double xi = t.xi_m, eta = t.eta_m, ke = t.ke_m;
+            s2 = t.scale;
+            s1 = nh_half(bx, xi, eta, ke);
+            if (i == bx.first) {
+                a.nh[b].xi_s = xi;
+                a.nh[b].eta_s = eta;
+            }
         }
         const float4 f = a.acc[i];
         const float acc[3] = {f.x, f.y, f.z};
@@ -368,6 +375,7 @@ __global__ void __launch_bounds__(kBlock) nh_begin_kernel(Arena a) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const size_t q = (size_t)k * a.seg + i;
+            // the two half steps' scalings in turn, then the half kick
             const double v = a.v[q] * s2 * s1 + (double)acc[k] * bx.half_dt;
             const double x = wrap(a.x[q] + v * bx.dt, bx.box[k]);
             a.x[q] = x;
@@ -382,61 +390,142 @@ __global__ void __launch_bounds__(kBlock) nh_begin_kernel(Arena a) {
     if (i == 0) a.glob->pending = 1u;
 }
 
-// nh_force: forces from the list, the closing half kick (not with PRIME,
-// which only records the first forces), and the kinetic energy summed exactly
-// in 32.32 fixed point; the last block to add its part does the end half
-// step's thermostat update (with PRIME: records the starting kinetic energy).
-template <bool SHIFTED_FORCE, bool PRIME>
-__global__ void __launch_bounds__(kForceThreads) nh_force_kernel(Arena a,
-                                                                 const __grid_constant__ CUtensorMap map) {
+// The exchange slab of height z (f32, as the reference): 0 hot, 1 cold, 2 neither.
+__device__ __forceinline__ int hex_slab(const Box& bx, double z) {
+    const float zf = (float)z;
+    if (zf >= bx.hex_slabs[0] && zf < bx.hex_slabs[1]) return 0;
+    if (zf >= bx.hex_slabs[2] && zf < bx.hex_slabs[3]) return 1;
+    return 2;
+}
+
+// The exchange's per-slab scale and eHEX/a correction coefficients from the
+// slab sums (lennard_jones.wgsl:804-856), in f64; clears the sums.
+__device__ void hex_coefficients(const Box& bx, Exchange* h) {
+    const double one = 4294967296.0;
+    const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
+    const double dt = bx.dt, dt3 = dt * dt * dt;
+    for (int sl = 0; sl < 2; sl++) {
+        long long raw[9];
+        for (int k = 0; k < 9; k++) {
+            raw[k] = (long long)h->sums[sl][k];
+            h->sums[sl][k] = 0ull;
+        }
+        const double m = (double)raw[0] / one;
+        double p[3], f[3];
+        for (int k = 0; k < 3; k++) {
+            p[k] = (double)raw[1 + k] / one / ms;
+            f[k] = (double)raw[6 + k] / one / ms;
+        }
+        const double v2 = (double)raw[4] / one / es, fv = (double)raw[5] / one / es;
+        double com[3] = {0.0, 0.0, 0.0}, mf[3] = {0.0, 0.0, 0.0};
+        double sm1 = 0.0, cv = 0.0, cf = 0.0;
+        if (m > 0.0) {
+            for (int k = 0; k < 3; k++) {
+                com[k] = p[k] / m;
+                mf[k] = f[k] / m;
+            }
+            // kinetic energy about the centre of mass
+            const double kinetic = 0.5 * v2 - 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / m;
+            const double energy = (sl == 0 ? 1.0 : -1.0) * bx.hex_energy;
+            const double flux = energy / dt;
+            const double x = energy / kinetic;
+            sm1 = x / (1.0 + sqrt(1.0 + x));  // sqrt(1 + x) - 1
+            const double power = fv - (f[0] * com[0] + f[1] * com[1] + f[2] * com[2]);
+            cv = dt3 * flux / (2.0 * kinetic * kinetic) * (flux / 48.0 + power / 6.0);
+            cf = dt3 * flux / (12.0 * kinetic);
+        }
+        for (int k = 0; k < 3; k++) {
+            h->com[sl][k] = com[k];
+            h->mean_f[sl][k] = mf[k];
+        }
+        h->s_minus_1[sl] = sm1;
+        h->c_v[sl] = cv;
+        h->c_f[sl] = cf;
+    }
+}
+
+// canon_force: forces from the list, stored; the closing half kick (not for
+// kPrime); the end-of-step sums in 32.32 fixed point, added per block, and in
+// the last block to finish the Nose-Hoover update or the exchange
+// coefficients.
+template <bool SHIFTED_FORCE, int PASS>
+__global__ void __launch_bounds__(kForceThreads) canon_force_kernel(Arena a,
+                                                                    const __grid_constant__ CUtensorMap map) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
-    __shared__ long long s_ke[kForceThreads / 32];
+    __shared__ unsigned long long s_sum[2][9];
     __shared__ int s_last;
     const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
     const bool valid = i < a.nslots;
     const Box& bx = a.boxes[0];
+    if (threadIdx.x < 18) s_sum[threadIdx.x / 9][threadIdx.x % 9] = 0ull;
     const PairSums s =
         block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, valid, a.cache[a.glob->phase]);
-    long long raw = 0;
     if (valid) {
         const float acc[3] = {s.ax, s.ay, s.az};
         a.acc[i] = make_float4(s.ax, s.ay, s.az, 0.0f);
-        double ke = 0.0;
+        double v[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const size_t q = (size_t)k * a.seg + i;
-            double v = a.v[q];
-            if (!PRIME) {
-                v += (double)acc[k] * bx.half_dt;
-                a.v[q] = v;
+            v[k] = a.v[q];
+            if (PASS != kPrime) {
+                v[k] += (double)acc[k] * bx.half_dt;
+                a.v[q] = v[k];
             }
-            ke += v * v;
         }
-        raw = fixed_raw_f64(0.5 * ke * (double)bx.energy_scale);
+        const double es = (double)bx.energy_scale, ms = (double)bx.momentum_scale;
+        if (PASS == kPrime || PASS == kNoseHoover) {
+            const long long raw = fixed_raw_f64(0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * es);
+            if (raw) atomicAdd(&s_sum[0][0], (unsigned long long)raw);
+        }
+        if (PASS == kExchange) {
+            const int sl = hex_slab(bx, a.x[2 * (size_t)a.seg + i]);
+            if (sl < 2) {
+                unsigned long long* t = s_sum[sl];
+                atomicAdd(&t[0], 1ull << 32);
+                for (int k = 0; k < 3; k++) {
+                    atomicAdd(&t[1 + k], (unsigned long long)fixed_raw_f64(v[k] * ms));
+                    atomicAdd(&t[6 + k], (unsigned long long)fixed_raw_f64((double)acc[k] * ms));
+                }
+                atomicAdd(&t[4], (unsigned long long)fixed_raw_f64(
+                                     (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * es));
+                atomicAdd(&t[5], (unsigned long long)fixed_raw_f64(
+                                     ((double)acc[0] * v[0] + (double)acc[1] * v[1] +
+                                      (double)acc[2] * v[2]) * es));
+            }
+        }
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) raw += __shfl_xor_sync(0xffffffffu, raw, o);
-    if (lane == 0) s_ke[warp] = raw;
+    if (PASS == kKick) return;
     __syncthreads();
     if (threadIdx.x == 0) {
-        long long sum = 0;
-        for (int w = 0; w < kForceThreads / 32; w++) sum += s_ke[w];
-        Thermo* t = a.nh;
-        if (sum) atomicAdd(&t->ke_raw, (unsigned long long)sum);
+        uint32_t* done;
+        if (PASS == kExchange) {
+            for (int sl = 0; sl < 2; sl++)
+                for (int k = 0; k < 9; k++)
+                    if (s_sum[sl][k]) atomicAdd(&a.hex->sums[sl][k], s_sum[sl][k]);
+            done = &a.hex->blocks_done;
+        } else {
+            if (s_sum[0][0]) atomicAdd(&a.nh->ke_raw, s_sum[0][0]);
+            done = &a.nh->blocks_done;
+        }
         __threadfence();
-        s_last = atomicAdd(&t->blocks_done, 1u) == gridDim.x - 1u;
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1u;
     }
     __syncthreads();
     if (!s_last || threadIdx.x != 0) return;
-    // every other block's kinetic energy is in: the thermostat update
+    // every other block's sums are in
     __threadfence();
+    if (PASS == kExchange) {
+        a.hex->blocks_done = 0u;
+        hex_coefficients(bx, a.hex);
+        return;
+    }
     Thermo* t = a.nh;
     const long long total = (long long)atomicExch(&t->ke_raw, 0ull);
     t->blocks_done = 0u;
     double ke = (double)total / 4294967296.0 / (double)bx.energy_scale;
-    if (PRIME) {
+    if (PASS == kPrime) {
         t->ke_m = ke;
         t->scale = 1.0;
         return;
@@ -447,6 +536,47 @@ __global__ void __launch_bounds__(kForceThreads) nh_force_kernel(Arena a,
     t->eta_m = eta;
     t->ke_m = ke;
     t->scale = s2;
+}
+
+// hex_apply (lennard_jones.wgsl:858-893): in each slab, the position
+// correction -dt^3 E_i from the velocity before scaling, then
+// v <- v + (s - 1)(v - v_com); the moved positions go back into the current
+// position copy.
+__global__ void __launch_bounds__(kBlock) hex_apply_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[0];
+    const int sl = hex_slab(bx, a.x[2 * (size_t)a.seg + i]);
+    if (sl == 2) return;
+    const Exchange& h = *a.hex;
+    const float4 f = a.acc[i];
+    const float acc[3] = {f.x, f.y, f.z};
+    uint32_t enc[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const size_t q = (size_t)k * a.seg + i;
+        const double v = a.v[q];
+        const double rel = v - h.com[sl][k];
+        const double shift = h.c_v[sl] * rel - h.c_f[sl] * ((double)acc[k] - h.mean_f[sl][k]);
+        const double x = wrap(a.x[q] - shift, bx.box[k]);
+        a.x[q] = x;
+        a.v[q] = v + h.s_minus_1[sl] * rel;
+        enc[k] = encode(x, bx.enc[k]);
+    }
+    a.cache[a.glob->phase][i] = make_uint4(enc[0], enc[1], enc[2], 0u);
+}
+
+// Canonical velocities back to half a kick behind, with the stored forces.
+__global__ void __launch_bounds__(kBlock) half_kick_back_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[0];
+    const float4 f = a.acc[i];
+    a.v[i] -= (double)f.x * bx.half_dt;
+    a.v[a.seg + i] -= (double)f.y * bx.half_dt;
+    a.v[2 * (size_t)a.seg + i] -= (double)f.z * bx.half_dt;
 }
 
 // ---- FP32 calibration: eight independent FMA chains per thread, so the
@@ -498,25 +628,42 @@ cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_
     return after_launch();
 }
 
-cudaError_t launch_nh_begin(const Arena& a, cudaStream_t s) {
-    nh_begin_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+cudaError_t launch_begin(const Arena& a, cudaStream_t s) {
+    begin_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
     return after_launch();
 }
 
-cudaError_t launch_nh_force(const Arena& a, const CUtensorMap& map, bool shifted_force, bool prime,
-                            cudaStream_t s) {
+template <bool SF>
+static void canon_force(const Arena& a, const CUtensorMap& map, CanonPass pass, cudaStream_t s) {
     const unsigned blocks = particle_blocks(a);
-    if (shifted_force) {
-        if (prime)
-            nh_force_kernel<true, true><<<blocks, kForceThreads, 0, s>>>(a, map);
-        else
-            nh_force_kernel<true, false><<<blocks, kForceThreads, 0, s>>>(a, map);
-    } else {
-        if (prime)
-            nh_force_kernel<false, true><<<blocks, kForceThreads, 0, s>>>(a, map);
-        else
-            nh_force_kernel<false, false><<<blocks, kForceThreads, 0, s>>>(a, map);
+    switch (pass) {
+        case kPrime: canon_force_kernel<SF, kPrime><<<blocks, kForceThreads, 0, s>>>(a, map); break;
+        case kNoseHoover:
+            canon_force_kernel<SF, kNoseHoover><<<blocks, kForceThreads, 0, s>>>(a, map);
+            break;
+        case kExchange:
+            canon_force_kernel<SF, kExchange><<<blocks, kForceThreads, 0, s>>>(a, map);
+            break;
+        case kKick: canon_force_kernel<SF, kKick><<<blocks, kForceThreads, 0, s>>>(a, map); break;
     }
+}
+
+cudaError_t launch_canon_force(const Arena& a, const CUtensorMap& map, bool shifted_force,
+                               CanonPass pass, cudaStream_t s) {
+    if (shifted_force)
+        canon_force<true>(a, map, pass, s);
+    else
+        canon_force<false>(a, map, pass, s);
+    return after_launch();
+}
+
+cudaError_t launch_hex_apply(const Arena& a, cudaStream_t s) {
+    hex_apply_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_half_kick_back(const Arena& a, cudaStream_t s) {
+    half_kick_back_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
     return after_launch();
 }
 

@@ -62,6 +62,7 @@ struct Box {
     double dt, half_dt;
     double c1, c2;       // Langevin v <- c1 v + c2 xi (lennard_jones.rs:520-523)
     double nh_gkt, nh_q; // Nose-Hoover g k T and Q (lennard_jones.rs:516-528)
+    double hex_energy;   // heat exchange: energy moved per step (its f32 value)
     float dec[3];        // side / 2^32, exact in f32
     float box_f[3];
     float cell_size_f[3];
@@ -70,6 +71,7 @@ struct Box {
     float energy_scale, momentum_scale;
     float bin_width;
     float inv_box_f[3];  // 1 / box_f, for nearest_ref_fast
+    float hex_slabs[4];  // heat exchange: hot lo, hi, cold lo, hi in z
     float prefilter_r2;  // list_r2 widened past any encoding difference
     float accept_r2;     // list_r2 narrowed past any encoding difference
     float reach_r2;      // prefilter_r2 widened past binning round-off
@@ -85,7 +87,8 @@ struct Box {
     uint32_t drawn;
     uint32_t reorder_every;
     uint32_t profile_bins;
-    uint32_t pad[2];
+    uint32_t canonical;  // velocities stored canonical (Nose-Hoover, heat exchange)
+    uint32_t pad;
 };
 
 // Mutable per-box words.
@@ -131,6 +134,21 @@ struct Thermo {
     uint32_t pad;
 };
 
+// Heat exchange state of a box (eHEX/a, lennard_jones.wgsl:732-893): per
+// slab (0 hot, 1 cold) the force pass's exact sums -- count, momentum (3),
+// sum of v^2, sum of f . v, sum of f (3) -- in 32.32 fixed point (momentum
+// and force times the momentum scale, the others times the energy scale),
+// then what the last block to finish works out of them for the apply pass.
+struct Exchange {
+    unsigned long long sums[2][9];
+    double com[2][3];     // centre-of-mass velocity
+    double mean_f[2][3];  // mean force
+    double s_minus_1[2];  // velocity scale about the centre of mass, minus one
+    double c_v[2], c_f[2];  // eq. 20's position-correction coefficients
+    uint32_t blocks_done;
+    uint32_t pad;
+};
+
 // Fault codes in Global::fault (the first one recorded wins).
 constexpr uint32_t kFaultTmaTimeout = 1;  // a TMA tile never arrived
 
@@ -173,8 +191,10 @@ struct Arena {
     double* sv;
     uint32_t* sid;
     uint32_t* scell;
-    // Nose-Hoover (null without): per-box state, and the last forces
+    // steps on canonical velocities (Nose-Hoover, heat exchange): the
+    // thermostat and exchange state, and the last forces
     Thermo* nh;
+    Exchange* hex;
     float4* acc;
     // measurements
     unsigned long long* accum;  // nboxes * kSlots
@@ -332,13 +352,19 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifte
                         cudaStream_t s);
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                            bool canonical, cudaStream_t s);
-// Nose-Hoover steps (one box): nh_begin scales (pending s2 and this step's
-// s1), kicks and drifts; nh_force computes the forces, kicks, and does the end
-// half step's thermostat update. With `prime` nh_force only computes the first
-// forces and the starting kinetic energy.
-cudaError_t launch_nh_begin(const Arena& a, cudaStream_t s);
-cudaError_t launch_nh_force(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
-                            bool prime, cudaStream_t s);
+// Steps on canonical velocities (one box): begin applies Nose-Hoover's
+// pending scale s2 and this step's s1, kicks and drifts; canon_force computes
+// the forces and then, by `pass`: kPrime records them (and the starting
+// kinetic energy) without a kick; kNoseHoover kicks and does the end half
+// step's thermostat update; kExchange kicks and sums the exchange slabs;
+// kKick only kicks. hex_apply moves the energy between the slabs.
+enum CanonPass { kPrime = 0, kNoseHoover = 1, kExchange = 2, kKick = 3 };
+cudaError_t launch_begin(const Arena& a, cudaStream_t s);
+cudaError_t launch_canon_force(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
+                               CanonPass pass, cudaStream_t s);
+cudaError_t launch_hex_apply(const Arena& a, cudaStream_t s);
+// Back from canonical velocities to half a kick behind (v -= a dt / 2).
+cudaError_t launch_half_kick_back(const Arena& a, cudaStream_t s);
 // Sampling kernels (vlj_sampling.cu): one profile sample added into
 // a.profile, one heat-current sample into a.series slot 1 + 3 * sample.
 cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cudaStream_t s);

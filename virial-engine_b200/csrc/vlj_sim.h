@@ -37,7 +37,10 @@ struct vlj_sim {
     vlj_settings settings{};
     uint32_t n = 0;
     bool shifted_force = false;
-    bool nose_hoover = false;  // steps run nh_begin / decide / rebuild / nh_force
+    bool nose_hoover = false;  // steps on canonical velocities with the thermostat
+    bool exchange = false;     // heat exchange on (constant energy, canonical velocities)
+    vlj_heat_exchange exchange_settings{};
+    bool canonical() const { return nose_hoover || exchange; }
     vlj::Box box{};
     // batched: one Box per replica, in slot order (empty for a single box)
     std::vector<vlj::Box> replicas;
