@@ -304,6 +304,9 @@ VLJ_API vlj_status vlj_debug_read_partials(vlj_sim *sim, float *pe_half, float *
 VLJ_API vlj_status vlj_debug_launches(uint64_t *launches);
 /* Kernels of this simulation that ran on the device (waits). */
 VLJ_API vlj_status vlj_debug_kernels_executed(vlj_sim *sim, uint64_t *kernels);
+/* The last measurement's per-particle float4 (vx, vy, vz, drawn value), in
+ * input order (n x 4 floats); waits. */
+VLJ_API vlj_status vlj_debug_read_vel4(vlj_sim *sim, float *out);
 /* 0: enqueue steps as direct launches instead of CUDA graphs. */
 VLJ_API vlj_status vlj_debug_set_graphs(vlj_sim *sim, int on);
 /* While on, steps are direct launches with CUDA events around every launch

@@ -178,3 +178,28 @@ def test_sampling_errors(gpu, O):
     with pytest.raises(gpu.VljError, match="record_heat_current"):
         sim.sample_heat_current()
     sim.clear_profile()  # nothing to clear: fine
+
+
+@pytest.mark.parametrize("drawn", ["NEIGHBOURS", "TEMPERATURE"])
+def test_drawn_values(gpu, O, drawn):
+    # lennard_jones.wgsl:595-602: neighbours within 1.5 sigma, or the local
+    # temperature over the particle and its neighbours within the cutoff
+    pos, vel = O.lattice(1000, 11.0, 1.0, 3)
+    sim = make(gpu, jitter(pos), vel, [11.0] * 3, shifted_force=False)
+    sim.run(50)
+    sim.set_drawn(getattr(gpu.Drawn, drawn))
+    sim.measure_now()
+    got = sim.read_vel4()
+    wp, v, box = canonical(sim)
+    d = wp[None, :, :] - wp[:, None, :]
+    d -= box * np.round(d / box)
+    r2 = (d ** 2).sum(-1)
+    np.fill_diagonal(r2, np.inf)
+    assert np.allclose(got[:, :3], v, rtol=1e-6, atol=1e-6)
+    if drawn == "NEIGHBOURS":
+        assert np.array_equal(got[:, 3], (r2 < 2.25).sum(1).astype(np.float32))
+    else:
+        near = r2 < 6.25
+        v2 = (v ** 2).sum(1)
+        want = (v2 + (near * v2[None, :]).sum(1)) / (3.0 * (near.sum(1) + 1))
+        assert np.allclose(got[:, 3], want, rtol=2e-5)

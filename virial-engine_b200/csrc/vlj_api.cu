@@ -271,6 +271,7 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
     CUDA_TRY(cudaMemsetAsync(s->arena.accum, 0, sizeof(unsigned long long) * kSlots, s->stream));
     TRY(lists_now(s));
     CUDA_TRY(launch_measure(s->arena, s->list_map, s->shifted_force, canonical, s->stream));
+    if (s->box.drawn == VLJ_DRAWN_TEMPERATURE) CUDA_TRY(launch_drawn_temperature(s->arena, s->stream));
     if (slot >= 0) {
         Readback* r = &s->ring[slot];
         CUDA_TRY(cudaMemcpyAsync(r->slots, s->arena.accum, sizeof(r->slots), cudaMemcpyDeviceToHost,
@@ -680,6 +681,25 @@ vlj_status vlj_debug_read_partials(vlj_sim* s, float* pe_half, float* w_half, in
                             cudaMemcpyDeviceToHost));
     if (raw)
         CUDA_TRY(cudaMemcpy(raw, s->arena.accum, sizeof(int64_t) * kSlots, cudaMemcpyDeviceToHost));
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_read_vel4(vlj_sim* s, float* out) {
+    if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
+    const size_t n = s->n;
+    std::vector<float4> v(n);
+    std::vector<uint32_t> id(n);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(cudaMemcpy(v.data(), s->arena.vel4, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(id.data(), s->arena.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    for (size_t slot = 0; slot < n; slot++) {
+        if (id[slot] >= n) return fail(VLJ_CUDA_ERROR, "corrupt particle id %u", id[slot]);
+        float* o = out + 4 * (size_t)id[slot];
+        o[0] = v[slot].x;
+        o[1] = v[slot].y;
+        o[2] = v[slot].z;
+        o[3] = v[slot].w;
+    }
     return VLJ_OK;
 }
 

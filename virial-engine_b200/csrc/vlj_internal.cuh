@@ -368,6 +368,9 @@ cudaError_t launch_half_kick_back(const Arena& a, cudaStream_t s);
 // Sampling kernels (vlj_sampling.cu): one profile sample added into
 // a.profile, one heat-current sample into a.series slot 1 + 3 * sample.
 cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cudaStream_t s);
+// After a measurement, each particle's local temperature into vel4.w:
+// m v^2 / 3 averaged over it and its neighbours within the cutoff.
+cudaError_t launch_drawn_temperature(const Arena& a, cudaStream_t s);
 cudaError_t launch_heat_current(const Arena& a, bool shifted_force, uint32_t sample,
                                 cudaStream_t s);
 cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s);

@@ -180,6 +180,38 @@ __global__ void __launch_bounds__(kSampleThreads) heat_current_kernel(Arena a, u
     }
 }
 
+// ---- drawn local temperature (lennard_jones.wgsl:595-602) ----
+// Runs after the measure kernel, which left each particle's canonical
+// velocity in vel4.xyz: (v_i^2 + sum over neighbours within the cutoff of
+// v_j^2) / (3 (neighbours + 1)), into vel4.w.
+__global__ void __launch_bounds__(kSampleThreads) drawn_temperature_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[box_of_slot(a, i)];
+    const uint4* __restrict__ cur = a.cache[a.glob->phase];
+    const uint4 own = cur[i];
+    const uint32_t cnt = a.list_count[i];
+    float v2 = 0.0f;
+    uint32_t within = 0;
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t j = a.list[((size_t)(k >> 2) * a.seg + i) * 4u + (k & 3u)];
+        if (encoded_r2(cur[j], own, bx.dec) < bx.rc2) {
+            const float4 vj = a.vel4[j];
+            v2 += vj.x * vj.x + vj.y * vj.y + vj.z * vj.z;
+            within += 1u;
+        }
+    }
+    float4 vi = a.vel4[i];
+    vi.w = (vi.x * vi.x + vi.y * vi.y + vi.z * vi.z + v2) / (3.0f * (float)(within + 1u));
+    a.vel4[i] = vi;
+}
+
+cudaError_t launch_drawn_temperature(const Arena& a, cudaStream_t s) {
+    drawn_temperature_kernel<<<blocks_for(a.nslots, kSampleThreads), kSampleThreads, 0, s>>>(a);
+    return after_launch();
+}
+
 cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cudaStream_t s) {
     const size_t words = (size_t)bins * kProfileSlots + 3;
     const size_t bytes = words * sizeof(unsigned long long);

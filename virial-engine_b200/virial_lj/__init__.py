@@ -448,6 +448,12 @@ class LennardJones:
         _check(_lib.vlj_debug_kernels_executed(self._h, C.byref(n)))
         return n.value
 
+    def read_vel4(self):
+        """The last measurement's (vx, vy, vz, drawn value) per particle, input order."""
+        out = np.zeros((self._n, 4), np.float32)
+        _check(_lib.vlj_debug_read_vel4(self._h, _ffi.ptr(out)))
+        return out
+
     def force_rebuild(self):
         _check(_lib.vlj_debug_force_rebuild(self._h))
 

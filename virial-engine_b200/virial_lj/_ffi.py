@@ -113,6 +113,7 @@ SIGNATURES = {
     "vlj_debug_launches": [_P(C.c_uint64)],
     "vlj_debug_kernels_executed": [_vp, _P(C.c_uint64)],
     "vlj_debug_set_graphs": [_vp, C.c_int],
+    "vlj_debug_read_vel4": [_vp, _vp],
     "vlj_debug_kernel_timing": [_vp, C.c_int],
     "vlj_debug_kernel_time": [_vp, _P(C.c_double), _P(C.c_uint64)],
     "vlj_debug_fp32_peak": [_P(C.c_double)],
