@@ -1,14 +1,17 @@
 // CUDA kernels of the pair forces, the integrator and the measurements,
 // sm_100a.
 //
-// One thread per particle, 128 per block. The block's Verlet-list rows (a
-// row is four entries of a particle, 16 B) stream from HBM into shared memory
-// as TMA tiles of 4 rows x 128 particles, three tiles in flight per block, so
-// the list -- most of the step's HBM traffic -- moves asynchronously while
-// the threads work. Each thread reads one whole row per iteration (one 16 B
-// shared-memory load, conflict-free across the warp), issues the four
-// neighbour gathers through L1 together, then does the four pairs' arithmetic.
-// Reference kernels are cited at each kernel.
+// One thread per particle, 128 per block. Each thread reads its Verlet-list
+// rows (a row is four entries of a particle, 16 B; a warp's rows are 512
+// contiguous bytes) one ahead with loads that do not allocate in L1, issues
+// the four neighbour gathers of a row through L1 together, then does the four
+// pairs' arithmetic. The force kernels use almost no shared memory and ask for
+// the largest L1 carve-out, so the L1 holds the neighbourhood the gathers
+// reuse. (The alternative, VLJ_LIST_STREAM=0, stages the rows in shared memory
+// as TMA tiles of kTileRows rows x 128 particles on an mbarrier ring; the
+// tuner measured it 16-45 % slower on the 256k-atom box, because the tiles
+// take the shared memory the L1 needs.) Reference kernels are cited at each
+// kernel.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -18,6 +21,11 @@
 namespace vlj {
 
 constexpr uint32_t kTileBytes = kTileRows * kForceThreads * 16u;
+// Resident blocks per SM the step kernel's register budget is sized for.
+#ifndef VLJ_STEP_MIN_BLOCKS
+#define VLJ_STEP_MIN_BLOCKS 1
+#endif
+constexpr int kStepMinBlocks = VLJ_STEP_MIN_BLOCKS;
 constexpr unsigned long long kWaitLimitNs = 500000000ull;  // 0.5 s per TMA tile
 
 struct PairSums {
@@ -27,11 +35,27 @@ struct PairSums {
     uint32_t near;    // neighbours within 1.5 sigma
 };
 
-// Shared memory of a force-kernel block: the tile ring and its barriers.
+// Shared memory of a force-kernel block: the tile ring and its barriers
+// (none when the rows stream straight from global memory).
+#if VLJ_LIST_STREAM
+struct Stage {
+    unsigned long long unused;
+};
+#else
 struct Stage {
     uint4 rows[kTileSlots][kTileRows][kForceThreads];
     unsigned long long bar[kTileSlots];
 };
+#endif
+
+// A list row (four entries of one slot, 16 B) read once: no L1 allocation,
+// so the L1 keeps the neighbour positions the gathers reuse.
+__device__ __forceinline__ uint4 load_row_streaming(const uint4* p) {
+    uint4 r;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
+    return r;
+}
 
 // ---- TMA and mbarrier primitives (PTX, sm_90+) ----
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -98,6 +122,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
                                                     const Arena& a, const Box& bx, uint32_t i,
                                                     bool valid, const uint4* __restrict__ cur) {
     PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u};
+#if !VLJ_LIST_STREAM
     const uint32_t first = blockIdx.x * kForceThreads;
     const uint32_t rows = a.block_rows[blockIdx.x];
     const uint32_t tiles = (rows + kTileRows - 1u) / kTileRows;
@@ -109,6 +134,10 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     if (threadIdx.x == 0)
         for (uint32_t t = 0; t < tiles && t < (uint32_t)kTileSlots; t++)
             tile_load(map, &st.rows[t][0][0], &st.bar[t], (int)(first * 2u), (int)(t * kTileRows));
+#else
+    (void)st;
+    (void)map;
+#endif
 
     uint4 own = make_uint4(0u, 0u, 0u, 0u);
     uint32_t cnt = 0;
@@ -151,6 +180,26 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         }
     };
 
+#if VLJ_LIST_STREAM
+    // each thread its own rows, the next one in flight while it works on this
+    const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;
+    uint4 next = my_rows ? load_row_streaming(rowp) : make_uint4(0u, 0u, 0u, 0u);
+    for (uint32_t row = 0; row < my_rows; row++) {
+        const uint4 e = next;
+        if (row + 1u < my_rows) next = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
+        const uint32_t k = row * 4u;
+        const bool l1 = k + 1u < cnt, l2 = k + 2u < cnt, l3 = k + 3u < cnt;
+        const uint4 p0 = __ldg(cur + e.x);
+        const uint4 p1 = l1 ? __ldg(cur + e.y) : own;
+        const uint4 p2 = l2 ? __ldg(cur + e.z) : own;
+        const uint4 p3 = l3 ? __ldg(cur + e.w) : own;
+        accumulate(p0, true);
+        accumulate(p1, l1);
+        accumulate(p2, l2);
+        accumulate(p3, l3);
+    }
+    return s;
+#else
     bool lost = false;
     for (uint32_t t = 0; t < tiles; t++) {
         const uint32_t slot = t % kTileSlots;
@@ -195,6 +244,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         __syncthreads();
     }
     return s;
+#endif
 }
 
 // Langevin noise of a particle at a step: Philox-4x32-10 (Salmon et al.,
@@ -246,7 +296,7 @@ __global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
 // step's), and the largest squared displacement since the last list build
 // feeds the next step's rebuild decision.
 template <bool SHIFTED_FORCE>
-__global__ void __launch_bounds__(kForceThreads) step_kernel(Arena a,
+__global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Arena a,
                                                              const __grid_constant__ CUtensorMap map) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
@@ -601,8 +651,40 @@ static unsigned particle_blocks(const Arena& a) {
     return blocks_for(a.nslots, kForceThreads);
 }
 
+// With the list streamed from global memory the force kernels use no shared
+// memory to speak of; ask for the largest L1 (it caches the gathers).
+template <class K>
+static void prefer_l1(K kernel) {
+#if VLJ_LIST_STREAM
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+#else
+    (void)kernel;
+#endif
+}
+
+static void prefer_l1_once() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    prefer_l1(step_kernel<true>);
+    prefer_l1(step_kernel<false>);
+    prefer_l1(measure_kernel<true>);
+    prefer_l1(measure_kernel<false>);
+    prefer_l1(prime_kernel<true>);
+    prefer_l1(prime_kernel<false>);
+    prefer_l1(canon_force_kernel<true, kPrime>);
+    prefer_l1(canon_force_kernel<false, kPrime>);
+    prefer_l1(canon_force_kernel<true, kNoseHoover>);
+    prefer_l1(canon_force_kernel<false, kNoseHoover>);
+    prefer_l1(canon_force_kernel<true, kExchange>);
+    prefer_l1(canon_force_kernel<false, kExchange>);
+    prefer_l1(canon_force_kernel<true, kKick>);
+    prefer_l1(canon_force_kernel<false, kKick>);
+}
+
 cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_force,
                          cudaStream_t s) {
+    prefer_l1_once();
     if (shifted_force)
         prime_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     else
@@ -612,6 +694,7 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_fo
 
 cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
                         cudaStream_t s) {
+    prefer_l1_once();
     if (shifted_force)
         step_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     else
@@ -621,6 +704,7 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_for
 
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_force,
                            bool canonical, cudaStream_t s) {
+    prefer_l1_once();
     if (shifted_force)
         measure_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, canonical ? 1 : 0);
     else
@@ -650,6 +734,7 @@ static void canon_force(const Arena& a, const CUtensorMap& map, CanonPass pass, 
 
 cudaError_t launch_canon_force(const Arena& a, const CUtensorMap& map, bool shifted_force,
                                CanonPass pass, cudaStream_t s) {
+    prefer_l1_once();
     if (shifted_force)
         canon_force<true>(a, map, pass, s);
     else

@@ -48,6 +48,12 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #ifndef VLJ_TILE_SLOTS
 #define VLJ_TILE_SLOTS 3
 #endif
+// 1: each force-kernel thread streams its own list rows from global memory
+// with loads that do not allocate in L1 (leaving all of L1 to the gathers)
+// instead of the TMA tile ring in shared memory.
+#ifndef VLJ_LIST_STREAM
+#define VLJ_LIST_STREAM 1
+#endif
 constexpr int kForceThreads = 128;
 constexpr int kTileRows = VLJ_TILE_ROWS;
 constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block

@@ -1,8 +1,9 @@
-"""Autotuner for the force kernels' TMA tile ring.
+"""Autotuner for how the force kernels read the Verlet list.
 
 The list rows staged in shared memory and the L1 that serves the neighbour
 gathers share each SM's 256 KB, so the tile depth (rows per tile, tiles in
-flight) trades list-stream latency against gather hit rate. This builds one
+flight) trades list-stream latency against gather hit rate; the rows can also
+stream per thread from global memory without L1 allocation (no tiles). This builds one
 library per candidate into build/tune/ (git-ignored), times the step kernel on
 a workload in a child process per variant (CUDA events around every launch,
 L2 flushed between steps), and prints the ranking as JSON lines. Needs a GPU.
@@ -21,7 +22,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "build", "tune")
-CANDIDATES = [(1, 4), (1, 6), (2, 3), (2, 4), (4, 2), (4, 3), (8, 2)]
+# (rows per tile, tiles in flight); rows 0 streams the rows without TMA, with
+# the step kernel's registers sized for `slots` resident blocks per SM
+CANDIDATES = [(0, 1), (0, 12), (0, 14), (1, 4), (4, 3)]
 
 
 def child(lib, cells, steps):
@@ -50,6 +53,9 @@ def main():
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--child", default=None)
+    ap.add_argument("--no-build", action="store_true",
+                    help="time the variants already in build/tune (built elsewhere)")
+    ap.add_argument("--build-only", action="store_true", help="build the variants, time nothing")
     args = ap.parse_args()
     if args.child:
         child(args.child, args.cells, args.steps)
@@ -60,7 +66,12 @@ def main():
     results = []
     for rows, slots in CANDIDATES:
         lib = os.path.join(OUT_DIR, f"libvirial_lj_r{rows}_s{slots}.so")
-        build.build(defines={"VLJ_TILE_ROWS": rows, "VLJ_TILE_SLOTS": slots}, out=lib)
+        defines = ({"VLJ_LIST_STREAM": 1, "VLJ_STEP_MIN_BLOCKS": slots} if rows == 0 else
+                   {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": rows, "VLJ_TILE_SLOTS": slots})
+        if not args.no_build:
+            build.build(defines=defines, out=lib, force=True)
+        if args.build_only:
+            continue
         out = subprocess.run([sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
                               "--steps", str(args.steps)], capture_output=True, text=True)
         if out.returncode != 0:
