@@ -297,6 +297,12 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
             }
             const uint32_t kept = found < cap ? found : cap;
             if (home) {
+                // the last row's unused places hold the particle itself: a zero
+                // separation, which the force kernels skip, so they read whole
+                // rows without a per-entry count test
+                uint32_t* row_of_i = a.list + (size_t)i * 4u;
+                for (uint32_t k = kept; k & 3u; k++)
+                    row_of_i[(size_t)(k >> 2) * row_stride + (k & 3u)] = i;
                 a.list_count[i] = kept;
                 if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
                 a.snap[i] = own_enc;

@@ -148,12 +148,14 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     const uint32_t my_rows = (cnt + 3u) / 4u;
     const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
     const float fshift = bx.force_shift;
-    auto accumulate = [&](const uint4 pj, bool live) {
+    // The list's last row is padded with the particle itself, whose zero
+    // separation drops out here with the entries beyond the cutoff.
+    auto accumulate = [&](const uint4 pj) {
         const float dx = decode_diff(pj.x, own.x, dec0);
         const float dy = decode_diff(pj.y, own.y, dec1);
         const float dz = decode_diff(pj.z, own.z, dec2);
         const float r2 = dx * dx + dy * dy + dz * dz;
-        const bool in = live && r2 < rc2;
+        const bool in = r2 < rc2 && r2 > 0.0f;
         // branch-free: most list entries are inside the cutoff; the select
         // drops whatever the pair math gives for entries that are not
         const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
@@ -187,16 +189,14 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     for (uint32_t row = 0; row < my_rows; row++) {
         const uint4 e = next;
         if (row + 1u < my_rows) next = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
-        const uint32_t k = row * 4u;
-        const bool l1 = k + 1u < cnt, l2 = k + 2u < cnt, l3 = k + 3u < cnt;
         const uint4 p0 = __ldg(cur + e.x);
-        const uint4 p1 = l1 ? __ldg(cur + e.y) : own;
-        const uint4 p2 = l2 ? __ldg(cur + e.z) : own;
-        const uint4 p3 = l3 ? __ldg(cur + e.w) : own;
-        accumulate(p0, true);
-        accumulate(p1, l1);
-        accumulate(p2, l2);
-        accumulate(p3, l3);
+        const uint4 p1 = __ldg(cur + e.y);
+        const uint4 p2 = __ldg(cur + e.z);
+        const uint4 p3 = __ldg(cur + e.w);
+        accumulate(p0);
+        accumulate(p1);
+        accumulate(p2);
+        accumulate(p3);
     }
     return s;
 #else
@@ -214,16 +214,14 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
             if (row < my_rows) {
                 // one row: four entries, the last ones live only up to cnt
                 const uint4 e = st.rows[slot][r][threadIdx.x];
-                const uint32_t k = row * 4u;
-                const bool l1 = k + 1u < cnt, l2 = k + 2u < cnt, l3 = k + 3u < cnt;
                 const uint4 p0 = __ldg(cur + e.x);
-                const uint4 p1 = l1 ? __ldg(cur + e.y) : own;
-                const uint4 p2 = l2 ? __ldg(cur + e.z) : own;
-                const uint4 p3 = l3 ? __ldg(cur + e.w) : own;
-                accumulate(p0, true);
-                accumulate(p1, l1);
-                accumulate(p2, l2);
-                accumulate(p3, l3);
+                const uint4 p1 = __ldg(cur + e.y);
+                const uint4 p2 = __ldg(cur + e.z);
+                const uint4 p3 = __ldg(cur + e.w);
+                accumulate(p0);
+                accumulate(p1);
+                accumulate(p2);
+                accumulate(p3);
             }
         }
         __syncthreads();
@@ -653,10 +651,13 @@ static unsigned particle_blocks(const Arena& a) {
 
 // With the list streamed from global memory the force kernels use no shared
 // memory to speak of; ask for the largest L1 (it caches the gathers).
+#ifndef VLJ_L1_CARVEOUT
+#define VLJ_L1_CARVEOUT 4  // shared-memory carve-out hint, percent of the maximum (tuned)
+#endif
 template <class K>
 static void prefer_l1(K kernel) {
 #if VLJ_LIST_STREAM
-    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, VLJ_L1_CARVEOUT);
 #else
     (void)kernel;
 #endif

@@ -10,8 +10,8 @@ L2 flushed between steps), and prints the ranking as JSON lines. Needs a GPU.
 
     python virial-engine_b200/tune.py [--cells 40] [--steps 60]
 
-The winner becomes the default of VLJ_TILE_ROWS / VLJ_TILE_SLOTS in
-csrc/vlj_internal.cuh.
+The winner's settings become the defaults of VLJ_LIST_STREAM / VLJ_L1_CARVEOUT
+(csrc/vlj_internal.cuh, csrc/vlj_forces.cu) or VLJ_TILE_ROWS / VLJ_TILE_SLOTS.
 """
 
 import argparse
@@ -22,9 +22,17 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "build", "tune")
-# (rows per tile, tiles in flight); rows 0 streams the rows without TMA, with
-# the step kernel's registers sized for `slots` resident blocks per SM
-CANDIDATES = [(0, 1), (0, 12), (0, 14), (1, 4), (4, 3)]
+# name -> preprocessor overrides: rows streamed without L1 allocation under
+# shared-memory carve-out hints (percent), or the TMA tile ring (rows per tile,
+# tiles in flight)
+CANDIDATES = {
+    "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
+    "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
+    "stream_c8": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8},
+    "stream_c16": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 16},
+    "tma_r1_s4": {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": 1, "VLJ_TILE_SLOTS": 4},
+    "tma_r4_s3": {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": 4, "VLJ_TILE_SLOTS": 3},
+}
 
 
 def child(lib, cells, steps):
@@ -64,10 +72,8 @@ def main():
     import build
     os.makedirs(OUT_DIR, exist_ok=True)
     results = []
-    for rows, slots in CANDIDATES:
-        lib = os.path.join(OUT_DIR, f"libvirial_lj_r{rows}_s{slots}.so")
-        defines = ({"VLJ_LIST_STREAM": 1, "VLJ_STEP_MIN_BLOCKS": slots} if rows == 0 else
-                   {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": rows, "VLJ_TILE_SLOTS": slots})
+    for name, defines in CANDIDATES.items():
+        lib = os.path.join(OUT_DIR, f"libvirial_lj_{name}.so")
         if not args.no_build:
             build.build(defines=defines, out=lib, force=True)
         if args.build_only:
@@ -75,10 +81,10 @@ def main():
         out = subprocess.run([sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
                               "--steps", str(args.steps)], capture_output=True, text=True)
         if out.returncode != 0:
-            print(json.dumps({"rows": rows, "slots": slots, "error": out.stderr[-500:]}), flush=True)
+            print(json.dumps({"variant": name, "error": out.stderr[-500:]}), flush=True)
             continue
         r = json.loads(out.stdout.strip().splitlines()[-1])
-        r.update(rows=rows, slots=slots)
+        r.update(variant=name, defines=defines)
         results.append(r)
         print(json.dumps(r), flush=True)
     if results:
