@@ -1,0 +1,192 @@
+"""Physical checks on the CUDA path: the reference's own long-run GPU tests,
+restated with its inputs and bounds.
+
+- tests/thermodynamics.rs:152-214  gas relaxes to Maxwell-Boltzmann at constant energy
+- tests/thermodynamics.rs:234-293  dilute gas: ideal-gas law and the virial expansion
+- tests/thermodynamics.rs:328-378  Nose-Hoover samples the canonical ensemble
+- tests/coexistence.rs:236-360     force-shifted slab at NIST SAT-TMMC densities,
+                                   flat normal pressure; truncated-shifted surface
+                                   tension against Vrabec et al.
+
+The reference constants (NIST densities and pressure with their 95 % limits,
+the surface-tension correlation) are the ones its tests hard-code.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from test_oracle_known_answers import second_virial
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def mean_error(x):
+    x = np.asarray(x, dtype=np.float64)
+    return float(x.mean()), float(x.std(ddof=1) / math.sqrt(len(x)))
+
+
+def erf(x):
+    return math.erf(x)
+
+
+def ks_distance(speeds, t):
+    """Kolmogorov-Smirnov distance from Maxwell-Boltzmann at temperature t."""
+    v = np.sort(np.asarray(speeds))
+    n = len(v)
+    a = math.sqrt(t)
+    x = v / (a * math.sqrt(2.0))
+    cdf = np.array([erf(q) for q in x]) - math.sqrt(2.0 / math.pi) * (v / a) * np.exp(-x * x)
+    i = np.arange(n)
+    return float(np.maximum(np.abs(cdf - i / n), np.abs((i + 1) / n - cdf)).max())
+
+
+def test_gas_relaxes_to_maxwell_boltzmann_at_constant_energy(gpu):
+    n, density = 4096, 0.1
+    box = (n / density) ** (1 / 3)
+    p = gpu.lattice(n, box, 1.0, 5)
+    speed = math.sqrt(3.0 * 2.0)
+    p["vel"] = p["vel"] / np.linalg.norm(p["vel"], axis=1)[:, None] * speed
+    sim = gpu.LennardJones(p, gpu.Settings([box] * 3, cutoff=2.5, dt=0.004, skin=0.3))
+    start = sim.measure_now()
+    dof = 3 * n - 3
+    speeds = lambda: np.linalg.norm(sim.read_particles()["vel"], axis=1)
+    d_start = ks_distance(speeds(), start.temperature(dof))
+    sim.run(10_000)
+    pooled, temps = [], []
+    for _ in range(10):
+        sim.run(500)
+        pooled.append(speeds())
+        temps.append(sim.measure_now().temperature(dof))
+    end = sim.measure_now()
+    d_end = ks_distance(np.concatenate(pooled), float(np.mean(temps)))
+    drift = (end.energy() - start.energy()) / abs(start.energy())
+    print(f"KS {d_start:.3f} -> {d_end:.4f}, drift {drift:.2e}")
+    assert d_start > 0.2
+    assert d_end < 0.01
+    assert abs(drift) < 1e-4
+
+
+def test_dilute_gas_obeys_ideal_gas_law_and_virial_expansion(gpu):
+    n, density, temperature = 4096, 0.01, 2.0
+    box = (n / density) ** (1 / 3)
+    p = gpu.lattice(n, box, temperature, 9)
+    sim = gpu.LennardJones(p, gpu.Settings([box] * 3, cutoff=2.5, dt=0.005, skin=0.3,
+                                           thermostat=gpu.Langevin(temperature, 1.0, 7)))
+    sim.run(4_000)
+    dof = 3 * n
+    z = []
+    for _ in range(2000):
+        sim.run(20)
+        m = sim.measure_now()
+        rho = n / m.volume
+        z.append(m.pressure() / (rho * m.temperature(dof)))
+    z = np.array(z)
+    mean = float(z.mean())
+    batches = z.reshape(20, -1).mean(1)
+    error = float(batches.std(ddof=1) / math.sqrt(len(batches)))
+    predicted = 1.0 + second_virial(temperature, 2.5) * n / sim.volume()
+    print(f"Z = {mean:.5f} +/- {error:.5f}; 1 + B2 rho = {predicted:.5f}")
+    assert abs(mean - 1.0) < 0.01
+    assert abs(mean - predicted) < 4.0 * max(error, 1e-4)
+
+
+def test_nose_hoover_samples_the_canonical_ensemble(gpu):
+    n, temperature = 1000, 1.5
+    box = (n / 0.3) ** (1 / 3)
+    sim = gpu.LennardJones(gpu.lattice(n, box, 0.5, 21),
+                           gpu.Settings([box] * 3, cutoff=2.5, dt=0.002, shifted_force=True,
+                                        skin=0.3, thermostat=gpu.NoseHoover(temperature, 0.5)))
+    sim.run(10_000)
+    dof = 3 * n - 3
+    start = sim.measure_now()
+    temps = []
+    for _ in range(2000):
+        sim.run(20)
+        temps.append(sim.measure_now().temperature(dof))
+    end = sim.measure_now()
+    temps = np.array(temps)
+    mean = float(temps.mean())
+    ratio = float(temps.var(ddof=1)) / mean ** 2
+    canonical = 2.0 / dof
+    drift = (end.extended_energy() - start.extended_energy()) / abs(start.extended_energy())
+    print(f"mean T {mean:.4f}; Var/T^2 {ratio:.3e} vs {canonical:.3e}; drift {drift:.2e}")
+    assert abs(mean / temperature - 1.0) < 0.01
+    assert abs(ratio / canonical - 1.0) < 0.15
+    assert abs(drift) < 1e-4
+    assert end.list_overflow == 0
+
+
+MIDPOINT, MARGIN = 0.37, 6.0
+
+
+def analyse(p, gpu):
+    density = p.density()
+    normal = [t[2] for t in p.pressure_tensor()]
+    phases = p.phases(MIDPOINT, MARGIN)
+    assert len(p.interfaces(MIDPOINT)) == 2, "one slab of liquid"
+    mean = lambda values, phase: p.mean_in(values, phases, phase)
+    kinetic = sum(sum(s.kinetic) for s in p.slabs)
+    particles = sum(s.particles for s in p.slabs)
+    return dict(liquid=mean(density, gpu.Phase.LIQUID), vapour=mean(density, gpu.Phase.VAPOUR),
+                normal=p.total_pressure_tensor()[2],
+                by_region=[mean(normal, ph) for ph in
+                           (gpu.Phase.LIQUID, gpu.Phase.INTERFACE, gpu.Phase.VAPOUR)],
+                gamma=p.surface_tension(), temperature=kinetic / (3.0 * particles))
+
+
+def coexistence(gpu, shifted_force, blocks):
+    size = [30.0, 30.0, 60.0]
+    thickness = 24.0
+    p = gpu.lattice_box(15_600, [30.0, 30.0, thickness], 0.7, 7)
+    p["pos"][:, 2] += (size[2] - thickness) / 2.0
+    sim = gpu.LennardJones(p, gpu.Settings(size, cutoff=2.5, dt=0.005, skin=0.3,
+                                           shifted_force=shifted_force, profile_bins=240,
+                                           thermostat=gpu.NoseHoover(0.7, 0.5)))
+    sim.run(20_000)
+    out = []
+    for _ in range(blocks):
+        sim.clear_profile()
+        for _ in range(1000):
+            sim.step(20)
+            sim.sample_profile()
+        out.append(analyse(sim.read_profile(), gpu))
+    return out
+
+
+def summary(blocks, key, k=None):
+    return mean_error([b[key] if k is None else b[key][k] for b in blocks])
+
+
+def test_force_shifted_slab_coexists_at_nist_densities(gpu):
+    blocks = coexistence(gpu, True, 10)
+    liquid, vapour = summary(blocks, "liquid"), summary(blocks, "vapour")
+    p_n, t = summary(blocks, "normal"), summary(blocks, "temperature")
+    regions = [summary(blocks, "by_region", k) for k in range(3)]
+    print(f"T {t}; liquid {liquid}; vapour {vapour}; P_N {p_n}; regions {regions}")
+    # NIST SAT-TMMC, linear-force-shifted LJ at 2.5 sigma, T = 0.7 (95 % limits)
+    nist_liquid, nist_liquid_95 = 0.729309, 1.93161e-4
+    nist_vapour, nist_vapour_95 = 1.95113e-2, 1.67304e-6
+    nist_p, nist_p_95 = 1.18969e-2, 8.67525e-7
+
+    def agrees(m, reference, limit95):
+        x, e = m
+        return abs(x - reference) < 3.0 * math.sqrt(e * e + (limit95 / 2.0) ** 2)
+
+    assert abs(t[0] - 0.7) < 0.002
+    assert agrees(liquid, nist_liquid, nist_liquid_95)
+    assert agrees(vapour, nist_vapour, nist_vapour_95)
+    assert agrees(p_n, nist_p, nist_p_95)
+    for region in regions:
+        assert agrees(region, p_n[0], 2.0 * p_n[1]), "normal pressure not flat"
+
+
+def test_truncated_shifted_slab_has_published_surface_tension(gpu):
+    blocks = coexistence(gpu, False, 10)
+    gamma, t = summary(blocks, "gamma"), summary(blocks, "temperature")
+    # Vrabec, Kedia, Fuchs and Hasse, Mol. Phys. 104, 1509 (2006)
+    published = 2.08 * (1.0 - 0.7 / 1.0779) ** 1.21
+    print(f"T {t}; gamma {gamma} vs {published:.4f}")
+    assert abs(t[0] - 0.7) < 0.002
+    assert abs(gamma[0] / published - 1.0) < 0.05

@@ -210,6 +210,7 @@ vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
 }
 
 vlj_status lists_now(vlj_sim* s) {
+    if (s->use_graphs && !s->timing) return sim_launch_lists_graph(s);
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
     return VLJ_OK;
@@ -293,6 +294,7 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
 vlj_sim::~vlj_sim() {
     if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
     if (graph_one) cudaGraphExecDestroy(graph_one);
+    if (graph_lists) cudaGraphExecDestroy(graph_lists);
     if (capture_stream) cudaStreamDestroy(capture_stream);
     for (cudaEvent_t e : ev_start) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_end) cudaEventDestroy(e);
@@ -994,6 +996,35 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         TRY(end_capture(cs, launch_step_tail(s, cs), &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
+    return VLJ_OK;
+}
+
+vlj_status sim_launch_lists_graph(vlj_sim* s) {
+    if (!s->graph_lists) {
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaGraphCreate(&g, 0));
+        struct Guard {
+            cudaGraph_t g;
+            ~Guard() { cudaGraphDestroy(g); }
+        } guard{g};
+        cudaStream_t cs = s->capture_stream;
+        const auto mode = cudaStreamCaptureModeThreadLocal;
+        cudaGraphConditionalHandle h;
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t n_decide = nullptr, n_cond = nullptr;
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, mode));
+        TRY(end_capture(cs, launch_decide(s->arena, cs, h), &n_decide));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        CUDA_TRY(cudaGraphAddNode(&n_cond, g, &n_decide, 1, &cp));
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, cp.conditional.phGraph_out[0], nullptr, nullptr,
+                                               0, mode));
+        TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
+        CUDA_TRY(cudaGraphInstantiate(&s->graph_lists, g, 0));
+    }
+    CUDA_TRY(cudaGraphLaunch(s->graph_lists, s->stream));
     return VLJ_OK;
 }
 

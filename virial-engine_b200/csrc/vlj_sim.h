@@ -69,6 +69,7 @@ struct vlj_sim {
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph_chunk = nullptr;
     cudaGraphExec_t graph_one = nullptr;
+    cudaGraphExec_t graph_lists = nullptr;  // decide -> IF(rebuild){rebuild chain}
     // per-launch timing of the step kernel (direct launches while on)
     bool timing = false;
     std::vector<cudaEvent_t> ev_start, ev_end;
@@ -84,4 +85,6 @@ vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out);
 vlj_status sim_lists_now(vlj_sim* s);
 vlj_status check_fault(vlj_sim* s);
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
+// The decision and, when due, the rebuild as one graph launch.
+vlj_status sim_launch_lists_graph(vlj_sim* s);
 }  // namespace vlj
