@@ -7,6 +7,8 @@ restated with its inputs and bounds.
 - tests/coexistence.rs:236-360     force-shifted slab at NIST SAT-TMMC densities,
                                    flat normal pressure; truncated-shifted surface
                                    tension against Vrabec et al.
+- tests/heat.rs:236-400            thermal conductivity: Fourier's law under the
+                                   eHEX exchange against Green-Kubo
 
 The reference constants (NIST densities and pressure with their 95 % limits,
 the surface-tension correlation) are the ones its tests hard-code.
@@ -190,3 +192,104 @@ def test_truncated_shifted_slab_has_published_surface_tension(gpu):
     print(f"T {t}; gamma {gamma} vs {published:.4f}")
     assert abs(t[0] - 0.7) < 0.002
     assert abs(gamma[0] / published - 1.0) < 0.05
+
+
+# ---- thermal conductivity: Fourier's law against Green-Kubo (tests/heat.rs:236-400) ----
+
+HEAT_DT = 0.002
+
+
+def heat_settings(gpu, size, bins):
+    return gpu.Settings(size, cutoff=2.5, dt=HEAT_DT, shifted_force=True, skin=0.3,
+                        profile_bins=bins)
+
+
+def heat_liquid(gpu, size, t=1.0):
+    count = int(round(0.8442 * size[0] * size[1] * size[2]))
+    return gpu.lattice_box(count, size, t, 11)
+
+
+def slope(x, y):
+    return float(np.polyfit(np.asarray(x), np.asarray(y), 1)[0])
+
+
+def non_equilibrium(gpu, blocks):
+    """Hot slab at z 0..2, cold at 20..22 in a 10 x 10 x 40 box: per block the
+    conductivity, the mean temperature and the bow of the profile."""
+    size = [10.0, 10.0, 40.0]
+    sim = gpu.LennardJones(heat_liquid(gpu, size), heat_settings(gpu, size, 80))
+    sim.run(5_000)
+    sim.set_heat_exchange(gpu.HeatExchange(hot=(0.0, 2.0), cold=(20.0, 22.0), energy=0.04))
+    flux = sim.heat_flux()
+    sim.run(50_000)
+    out = []
+    for _ in range(blocks):
+        sim.clear_profile()
+        for _ in range(500):
+            sim.step(20)
+            sim.sample_profile()
+        p = sim.read_profile()
+        t = np.array(p.temperature())
+        z = np.array([s.z for s in p.slabs])
+
+        def fit(lo, hi):
+            m = (z > lo) & (z < hi)
+            return slope(z[m], t[m])
+
+        def mean(lo, hi):
+            m = (z > lo) & (z < hi)
+            return float(t[m].mean())
+
+        def bow(lo):
+            third = 10.0 / 3.0
+            a, b, c = mean(lo, lo + third), mean(lo + third, lo + 2 * third), mean(lo + 2 * third, lo + 10)
+            return (b - 0.5 * (a + c)) / abs(a - c)
+
+        gradient = 0.5 * (-fit(6.0, 16.0) + fit(26.0, 36.0))
+        out.append((flux / gradient, float(t.mean()), 0.5 * (bow(6.0) + bow(26.0))))
+    return out
+
+
+def green_kubo(gpu, blocks):
+    """lambda = 1 / (3 V T^2) integral of <J(0) . J(t)> dt at constant energy."""
+    size = [16.0, 16.0, 16.0]
+    sim = gpu.LennardJones(heat_liquid(gpu, size), heat_settings(gpu, size, 0))
+    sim.run(5_000)
+    n, volume = sim.count(), sim.volume()
+    every, samples = 2, 50_000
+    dt = HEAT_DT * every
+    lags = int(6.0 / dt)
+    out = []
+    for _ in range(blocks):
+        sim.record_heat_current(samples)
+        kinetic = 0.0
+        for s in range(samples):
+            sim.step(every)
+            sim.sample_heat_current()
+            if s % 500 == 499:
+                kinetic += sim.measure_now().kinetic
+        t = 2.0 * kinetic / (samples / 500) / (3.0 * n - 3.0)
+        j = sim.read_heat_current()
+        # <J(0) . J(t)> over time origins, by FFT
+        size_fft = 1 << (2 * samples - 1).bit_length()
+        corr = np.zeros(lags + 1)
+        for k in range(3):
+            f = np.fft.rfft(j[:, k], size_fft)
+            corr += np.fft.irfft(f * np.conj(f), size_fft)[: lags + 1]
+        corr /= (samples - np.arange(lags + 1))
+        integral = dt * (corr.sum() - 0.5 * (corr[0] + corr[lags]))
+        out.append((integral / (3.0 * volume * t * t), t))
+    return out
+
+
+def test_conductivity_from_fourier_law_agrees_with_green_kubo(gpu):
+    nemd = non_equilibrium(gpu, 8)
+    gk = green_kubo(gpu, 8)
+    l_nemd, e_nemd = mean_error([b[0] for b in nemd])
+    bow, e_bow = mean_error([b[2] for b in nemd])
+    l_gk, e_gk = mean_error([b[0] for b in gk])
+    combined = math.sqrt(e_nemd ** 2 + e_gk ** 2)
+    print(f"Fourier {l_nemd:.3f} +/- {e_nemd:.3f}; Green-Kubo {l_gk:.3f} +/- {e_gk:.3f}; "
+          f"bow {bow:+.3f} +/- {e_bow:.3f}")
+    assert abs(l_nemd - l_gk) < 3.0 * combined
+    assert abs(bow) < 3.0 * e_bow + 0.02
