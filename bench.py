@@ -402,10 +402,10 @@ def run_ours(args, world, rank, gpu_index):
     e2e_s = time.perf_counter() - t0
     e2e_max = reduce_max(world, e2e_s)
     e2e_value = world * n * E2E_INNER * e2e_steps / e2e_max
-    g = sim.grid_info()
-    seg = g.segment
-    h2d = seg * (24 + 24 + 4)
-    d2h = seg * (24 + 24 + 4) + 8 * 8 + 32
+    # the particle array each way (48 B per particle), plus the measurement's
+    # fixed-point sums and control words and the upload's status word
+    h2d = 48 * n
+    d2h = 48 * n + 8 * 8 + 32 + 48
 
     # ---- CPU baseline (rank 0, one GPU only) ----
     cpu = None

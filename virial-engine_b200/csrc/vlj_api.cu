@@ -178,34 +178,21 @@ vlj_status dalloc(vlj_sim* s, T** p, size_t count) {
     return VLJ_OK;
 }
 
-double rem_euclid(double x, double side) {
-    double r = std::fmod(x, side);
-    return r < 0.0 ? r + side : r;
-}
-
-// Positions (wrapped into the box) and velocities as structure-of-arrays
-// uploads; ids are the input order.
+// The particles as given (one copy of the caller's array), then on the
+// device: positions wrapped into the box, structure of arrays, ids the input
+// order. A non-finite coordinate is reported once the copy has landed.
 vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
-    const size_t seg = s->arena.seg;
-    double* x = s->pin_x;
-    double* v = s->pin_v;
-    uint32_t* id = s->pin_id;
-    for (size_t i = 0; i < count; i++) {
-        for (int k = 0; k < 3; k++) {
-            if (!std::isfinite(p[i].pos[k]) || !std::isfinite(p[i].vel[k]))
-                return fail(VLJ_INVALID_ARG, "particle %zu has a non-finite coordinate", i);
-            x[k * seg + i] = rem_euclid(p[i].pos[k], s->box.box[k]);
-            v[k * seg + i] = p[i].vel[k];
-        }
-        id[i] = (uint32_t)i;
-    }
-    CUDA_TRY(cudaMemcpyAsync(s->arena.x, x, sizeof(double) * 3 * seg, cudaMemcpyHostToDevice,
+    CUDA_TRY(cudaMemsetAsync(&s->arena.glob->fault, 0, sizeof(uint32_t), s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->arena.aos, p, sizeof(vlj_particle) * count, cudaMemcpyHostToDevice,
                              s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->arena.v, v, sizeof(double) * 3 * seg, cudaMemcpyHostToDevice,
-                             s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->arena.id, id, sizeof(uint32_t) * seg, cudaMemcpyHostToDevice,
-                             s->stream));
+    CUDA_TRY(launch_load_particles(s->arena, s->stream));
+    Global g;
+    CUDA_TRY(cudaMemcpyAsync(&g, s->arena.glob, sizeof g, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (g.fault == kFaultNonFinite) {
+        cudaMemsetAsync(&s->arena.glob->fault, 0, sizeof(uint32_t), s->stream);
+        return fail(VLJ_INVALID_ARG, "a particle has a non-finite coordinate");
+    }
     return VLJ_OK;
 }
 
@@ -439,26 +426,11 @@ vlj_status vlj_measure_now(vlj_sim* s, vlj_measurement* out) {
 vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
     if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
     TRY(enqueue_measure(s, true, -1));
-    const size_t seg = s->arena.seg;
-    double* x = s->pin_x;
-    double* v = s->pin_v;
-    uint32_t* id = s->pin_id;
-    CUDA_TRY(cudaMemcpyAsync(x, s->arena.x, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
-                             s->stream));
-    CUDA_TRY(cudaMemcpyAsync(v, s->arena.vcanon, sizeof(double) * 3 * seg, cudaMemcpyDeviceToHost,
-                             s->stream));
-    CUDA_TRY(cudaMemcpyAsync(id, s->arena.id, sizeof(uint32_t) * seg, cudaMemcpyDeviceToHost,
+    CUDA_TRY(launch_store_particles(s->arena, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(out, s->arena.aos, sizeof(vlj_particle) * s->n, cudaMemcpyDeviceToHost,
                              s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    for (uint32_t slot = 0; slot < s->n; slot++) {
-        uint32_t i = id[slot];
-        if (i >= s->n) return fail(VLJ_CUDA_ERROR, "corrupt particle id %u in slot %u", i, slot);
-        for (int k = 0; k < 3; k++) {
-            out[i].pos[k] = x[k * seg + slot];
-            out[i].vel[k] = v[k * seg + slot];
-        }
-    }
-    return VLJ_OK;
+    return check_fault(s);
 }
 
 vlj_status vlj_write_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
@@ -902,6 +874,7 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((cap + 3) / 4)));
     TRY(dalloc(s, &a.block_rows, ((size_t)seg + kForceThreads - 1) / kForceThreads));
     TRY(make_list_map(a, (cap + 3) / 4, &s->list_map));
+    TRY(dalloc(s, &a.aos, 6 * (size_t)seg));
     TRY(dalloc(s, &a.sx, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sv, 3 * (size_t)seg));
     TRY(dalloc(s, &a.sid, seg));

@@ -50,6 +50,40 @@ __global__ void encode_kernel(Arena a) {
     a.cache[a.glob->phase][i] = w;
 }
 
+// ---- particles in and out (lennard_jones.rs:1354-1374; input order) ----
+__global__ void load_particles_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    const Box& bx = a.boxes[0];
+    const double* p = a.aos + 6 * (size_t)i;
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double x = p[k], v = p[3 + k];
+        finite = finite && isfinite(x) && isfinite(v);
+        // rem_euclid: fmod is exact, so this is the host's result to the bit
+        double r = fmod(x, bx.box[k]);
+        if (r < 0.0) r += bx.box[k];
+        a.x[(size_t)k * a.seg + i] = r;
+        a.v[(size_t)k * a.seg + i] = v;
+    }
+    a.id[i] = i;
+    if (!finite) atomicCAS(&a.glob->fault, 0u, kFaultNonFinite);
+}
+
+__global__ void store_particles_kernel(Arena a) {
+    count_kernel(a);
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nslots) return;
+    double* p = a.aos + 6 * (size_t)a.id[s];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        p[k] = a.x[(size_t)k * a.seg + s];
+        p[3 + k] = a.vcanon[(size_t)k * a.seg + s];
+    }
+}
+
 // ---- decide (lennard_jones.wgsl:281-307) ----
 // One block. Finishes the previous step's bookkeeping (flip the position
 // copy, advance the step counter), then per box: rebuild when something moved
@@ -339,6 +373,16 @@ __global__ void pack_kernel(Arena a) {
 // ---- launchers ----
 cudaError_t launch_encode(const Arena& a, cudaStream_t s) {
     encode_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_load_particles(const Arena& a, cudaStream_t s) {
+    load_particles_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
+    return after_launch();
+}
+
+cudaError_t launch_store_particles(const Arena& a, cudaStream_t s) {
+    store_particles_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
     return after_launch();
 }
 

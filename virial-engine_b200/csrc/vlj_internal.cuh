@@ -157,6 +157,7 @@ struct Exchange {
 
 // Fault codes in Global::fault (the first one recorded wins).
 constexpr uint32_t kFaultTmaTimeout = 1;  // a TMA tile never arrived
+constexpr uint32_t kFaultNonFinite = 2;   // an uploaded coordinate was not finite
 
 // Every pointer a kernel needs; passed by value (it sits in the constant
 // bank), so captured graphs see fixed pointers and read the mutable state
@@ -192,6 +193,9 @@ struct Arena {
     // the box that holds the whole block; a block across two boxes keeps the
     // largest value it ever had (more rows staged, never fewer).
     uint32_t* block_rows;
+    // particles as the API passes them (pos[3], vel[3] per particle, input
+    // order), staged for upload and read-back
+    double* aos;
     // reorder scratch
     double* sx;
     double* sv;
@@ -346,6 +350,12 @@ __device__ __forceinline__ float encoded_r2(uint4 a, uint4 b, const float dec[3]
 
 // ---- launchers (vlj_kernels.cu); every kernel takes the Arena by value ----
 cudaError_t launch_encode(const Arena& a, cudaStream_t s);
+// Particles from a.aos (input order) into the state of a single box: positions
+// wrapped into the box, ids the input order; a non-finite coordinate records
+// kFaultNonFinite. And back: positions and canonical velocities (a.vcanon)
+// into a.aos in input order.
+cudaError_t launch_load_particles(const Arena& a, cudaStream_t s);
+cudaError_t launch_store_particles(const Arena& a, cudaStream_t s);
 cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle);
 cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
 // The force kernels read list rows through `list_map`: a 2D TMA tensor map
