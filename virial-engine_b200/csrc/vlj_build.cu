@@ -171,6 +171,10 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
             uint32_t found = 0;  // this lane's home particle's list length so far
             const uint32_t homes = min(hend - h0, 32u);
             uint32_t staged = 0;
+            // where a full cell's lane writes its next entry: the row, and the
+            // place in it (entry `found`, kept while found < cap)
+            uint32_t* wrow = a.list + (size_t)i * 4u;
+            uint32_t wcol = 0;
             for (uint32_t base = 0; base < total; base += kRound) {
                 // Fetch the next kRound candidates of the stream (kRound / 32 per
                 // lane, loads in flight together), keep those within reach of the
@@ -246,15 +250,37 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                     // Full cells: each lane tests its home particle against
                     // every staged candidate in stream order (one broadcast
                     // shared-memory read per candidate for the whole warp).
-                    uint32_t* row_of_i = a.list + (size_t)i * 4u;
-                    for (uint32_t q = 0; q < staged; q++) {
-                        const uint4 e = s_cand[warp][q];
-                        const float r2e = sep2(e, own_rel[0], own_rel[1], own_rel[2], own_enc);
-                        if (home && r2e < pre_r2 && e.w != i &&
-                            (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510))) {
-                            if (found < cap)
-                                row_of_i[(size_t)(found >> 2) * row_stride + (found & 3u)] = e.w;
-                            found += 1;
+                    // The common outcomes -- out, or in by the encoded test --
+                    // take a few instructions; the reference's own arithmetic
+                    // runs only in the thin shell.
+                    auto append = [&](uint32_t j) {
+                        if (found < cap) wrow[wcol] = j;
+                        found += 1;
+                        if (++wcol == 4u) {
+                            wcol = 0;
+                            wrow += row_stride;
+                        }
+                    };
+                    if (wide) {
+                        const float ox = own_rel[0], oy = own_rel[1], oz = own_rel[2];
+#pragma unroll 2
+                        for (uint32_t q = 0; q < staged; q++) {
+                            const uint4 e = s_cand[warp][q];
+                            const float dx = __uint_as_float(e.x) - ox;
+                            const float dy = __uint_as_float(e.y) - oy;
+                            const float dz = __uint_as_float(e.z) - oz;
+                            const float r2e = dx * dx + dy * dy + dz * dz;
+                            if (r2e < pre_r2 && e.w != i &&
+                                (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510)))
+                                append(e.w);
+                        }
+                    } else {
+                        for (uint32_t q = 0; q < staged; q++) {
+                            const uint4 e = s_cand[warp][q];
+                            const float r2e = encoded_r2(e, own_enc, dec);
+                            if (home && r2e < pre_r2 && e.w != i &&
+                                (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510)))
+                                append(e.w);
                         }
                     }
                 } else {
