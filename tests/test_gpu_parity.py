@@ -258,5 +258,6 @@ def test_kernel_counter_counts_skipped_rebuilds_out(gpu):
     sim.run(64)
     k1 = sim.kernels_executed()
     r1 = sim.measure_now().list_rebuilds
-    # two kernels per step plus seven per rebuild
-    assert k1 - k0 == 2 * 64 + 7 * (r1 - r0)
+    # a step kernel per step, a decide per 16-step graph (the step kernels take
+    # the later steps' decisions), seven per rebuild
+    assert k1 - k0 == 64 + 64 // 16 + 7 * (r1 - r0)

@@ -946,19 +946,27 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
     } guard{g};
     cudaStream_t cs = s->capture_stream;
     const auto mode = cudaStreamCaptureModeThreadLocal;
+    // one conditional per step; with the fused step kernel, step k's kernel
+    // takes step k + 1's decision, so only the first step launches decide
+    const bool fold = !s->canonical();
+    std::vector<cudaGraphConditionalHandle> h(count);
+    for (uint32_t k = 0; k < count; k++)
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
     cudaGraphNode_t prev = nullptr;
     for (uint32_t k = 0; k < count; k++) {
-        cudaGraphConditionalHandle h;
-        CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
         cudaGraphNode_t n_decide = nullptr, n_cond = nullptr;
-        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, prev ? &prev : nullptr, nullptr, prev ? 1 : 0,
-                                               mode));
-        cudaError_t e = cudaSuccess;
-        if (s->canonical()) e = launch_begin(s->arena, cs);
-        if (e == cudaSuccess) e = launch_decide(s->arena, cs, h);
-        TRY(end_capture(cs, e, &n_decide));
+        if (k == 0 || !fold) {
+            CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, prev ? &prev : nullptr, nullptr,
+                                                   prev ? 1 : 0, mode));
+            cudaError_t e = cudaSuccess;
+            if (s->canonical()) e = launch_begin(s->arena, cs);
+            if (e == cudaSuccess) e = launch_decide(s->arena, cs, h[k]);
+            TRY(end_capture(cs, e, &n_decide));
+        } else {
+            n_decide = prev;  // the previous step kernel decided
+        }
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-        cp.conditional.handle = h;
+        cp.conditional.handle = h[k];
         cp.conditional.type = cudaGraphCondTypeIf;
         cp.conditional.size = 1;
         CUDA_TRY(cudaGraphAddNode(&n_cond, g, &n_decide, 1, &cp));
@@ -966,7 +974,13 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
         TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
-        TRY(end_capture(cs, launch_step_tail(s, cs), &prev));
+        cudaError_t e;
+        if (fold)
+            e = launch_step(s->arena, s->list_map, s->shifted_force, cs,
+                            k + 1 < count ? (unsigned long long)h[k + 1] : 0ull);
+        else
+            e = launch_step_tail(s, cs);
+        TRY(end_capture(cs, e, &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
     return VLJ_OK;

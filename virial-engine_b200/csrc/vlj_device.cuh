@@ -36,6 +36,52 @@ __device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
     return a.ctrl[b].rebuild != 0u;
 }
 
+// ---- decide (lennard_jones.wgsl:281-307), by one whole block ----
+// Finishes the previous step's bookkeeping (flip the position copy, advance
+// the step counter), then per box: rebuild when something moved more than
+// skin / 2 since the last build, or never built; reorder on every
+// reorder_every-th rebuild (counted before the increment, as the reference).
+// With `set`, the verdict (some box rebuilds) becomes the value of the graph
+// conditional `handle`.
+__device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditionalHandle handle,
+                                             bool set) {
+    __shared__ int s_any;
+    Global* g = a.glob;
+    if (threadIdx.x == 0) {
+        s_any = 0;
+        g->work_cells = 0u;
+        g->next_build = 0u;
+        if (g->pending) {
+            g->phase ^= 1u;
+            g->step += 1ull;
+            g->pending = 0u;
+        }
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < a.nboxes; b += blockDim.x) {
+        Control& c = a.ctrl[b];
+        const Box& bx = a.boxes[b];
+        const float moved = __uint_as_float(c.max_disp);
+        c.max_disp = 0u;
+        const bool rebuild = moved > bx.half_skin2 || c.built == 0u || c.forced != 0u;
+        c.forced = 0u;
+        c.rebuild = rebuild ? 1u : 0u;
+        if (rebuild) {
+            c.reorder = (c.rebuilds % bx.reorder_every == 0u) ? 1u : 0u;
+            c.rebuilds += 1u;
+            c.built = 1u;
+            s_any = 1;
+        } else {
+            c.reorder = 0u;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g->any = (uint32_t)s_any;
+        if (set) cudaGraphSetConditional(handle, (unsigned)s_any);
+    }
+}
+
 // Whether every valid thread of the block belongs to the box of the block's
 // first slot; that box in *ref. Call from every thread of the block.
 __device__ __forceinline__ bool block_in_one_box(const Arena& a, bool valid, uint32_t b,

@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
 // feeds the next step's rebuild decision.
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Arena a,
-                                                             const __grid_constant__ CUtensorMap map) {
+                                                             const __grid_constant__ CUtensorMap map,
+                                                             cudaGraphConditionalHandle next) {
     count_kernel(a);
     __shared__ __align__(128) Stage st;
     const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
@@ -336,6 +337,19 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     }
     block_max_per_box(a, valid, b, blockIdx.x * kForceThreads, disp2);
     if (i == 0) a.glob->pending = 1u;
+    if (!next) return;
+    // the last block to finish takes the next step's rebuild decision
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&a.glob->blocks_done, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) a.glob->blocks_done = 0u;
+    decide_block(a, next, true);
 }
 
 // ---- measure (lennard_jones.wgsl:576-626) ----
@@ -694,12 +708,13 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_fo
 }
 
 cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
-                        cudaStream_t s) {
+                        cudaStream_t s, unsigned long long next_decision) {
     prefer_l1_once();
+    const cudaGraphConditionalHandle next = (cudaGraphConditionalHandle)next_decision;
     if (shifted_force)
-        step_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
+        step_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, next);
     else
-        step_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
+        step_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, next);
     return after_launch();
 }
 

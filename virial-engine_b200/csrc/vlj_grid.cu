@@ -92,41 +92,7 @@ __global__ void store_particles_kernel(Arena a) {
 template <bool SET_CONDITION>
 __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
     count_kernel(a);
-    __shared__ int s_any;
-    Global* g = a.glob;
-    if (threadIdx.x == 0) {
-        s_any = 0;
-        g->work_cells = 0u;
-        g->next_build = 0u;
-        if (g->pending) {
-            g->phase ^= 1u;
-            g->step += 1ull;
-            g->pending = 0u;
-        }
-    }
-    __syncthreads();
-    for (uint32_t b = threadIdx.x; b < a.nboxes; b += blockDim.x) {
-        Control& c = a.ctrl[b];
-        const Box& bx = a.boxes[b];
-        float moved = __uint_as_float(c.max_disp);
-        c.max_disp = 0u;
-        bool rebuild = moved > bx.half_skin2 || c.built == 0u || c.forced != 0u;
-        c.forced = 0u;
-        c.rebuild = rebuild ? 1u : 0u;
-        if (rebuild) {
-            c.reorder = (c.rebuilds % bx.reorder_every == 0u) ? 1u : 0u;
-            c.rebuilds += 1u;
-            c.built = 1u;
-            s_any = 1;
-        } else {
-            c.reorder = 0u;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        g->any = (uint32_t)s_any;
-        if (SET_CONDITION) cudaGraphSetConditional(handle, (unsigned)s_any);
-    }
+    decide_block(a, handle, SET_CONDITION);
 }
 
 // ---- bin (grid.wgsl:11-38): cell of each slot from its f32 position ----

@@ -120,7 +120,7 @@ struct Global {
     uint32_t max_count;          // longest list built so far
     uint32_t work_cells;         // entries of Arena::work this step
     uint32_t next_build;         // next work entry the list build takes
-    uint32_t pad;
+    uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).
@@ -364,8 +364,11 @@ cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
 // kForceThreads slots.
 cudaError_t launch_prime(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                          cudaStream_t s);
+// `next_decision`, when not 0, is the graph conditional of the next step's
+// rebuild: the step kernel's last block to finish then takes the next step's
+// decision itself (in place of a decide launch) and sets it.
 cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
-                        cudaStream_t s);
+                        cudaStream_t s, unsigned long long next_decision = 0);
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                            bool canonical, cudaStream_t s);
 // Steps on canonical velocities (one box): begin applies Nose-Hoover's
