@@ -183,8 +183,37 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     };
 
 #if VLJ_LIST_STREAM
-    // each thread its own rows, the next one in flight while it works on this
     const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;
+#if VLJ_GATHER_AHEAD
+    // gathers one row ahead: row r + 1's neighbours are in flight while row
+    // r's pairs are computed (its list row two ahead)
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    uint4 e_next = my_rows > 1u ? load_row_streaming(rowp + a.seg) : zero;
+    uint4 q0 = own, q1 = own, q2 = own, q3 = own;
+    if (my_rows) {
+        const uint4 e = load_row_streaming(rowp);
+        q0 = __ldg(cur + e.x);
+        q1 = __ldg(cur + e.y);
+        q2 = __ldg(cur + e.z);
+        q3 = __ldg(cur + e.w);
+    }
+    for (uint32_t row = 0; row < my_rows; row++) {
+        const uint4 p0 = q0, p1 = q1, p2 = q2, p3 = q3;
+        if (row + 1u < my_rows) {
+            const uint4 e = e_next;
+            if (row + 2u < my_rows) e_next = load_row_streaming(rowp + (size_t)(row + 2u) * a.seg);
+            q0 = __ldg(cur + e.x);
+            q1 = __ldg(cur + e.y);
+            q2 = __ldg(cur + e.z);
+            q3 = __ldg(cur + e.w);
+        }
+        accumulate(p0);
+        accumulate(p1);
+        accumulate(p2);
+        accumulate(p3);
+    }
+#else
+    // each thread its own rows, the next one in flight while it works on this
     uint4 next = my_rows ? load_row_streaming(rowp) : make_uint4(0u, 0u, 0u, 0u);
     for (uint32_t row = 0; row < my_rows; row++) {
         const uint4 e = next;
@@ -198,6 +227,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         accumulate(p2);
         accumulate(p3);
     }
+#endif
     return s;
 #else
     bool lost = false;

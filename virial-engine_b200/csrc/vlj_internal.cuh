@@ -54,6 +54,11 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #ifndef VLJ_LIST_STREAM
 #define VLJ_LIST_STREAM 1
 #endif
+// 1: with streamed rows, issue the next row's neighbour gathers before
+// computing this row's pairs (twice the loads in flight, more registers).
+#ifndef VLJ_GATHER_AHEAD
+#define VLJ_GATHER_AHEAD 0
+#endif
 constexpr int kForceThreads = 128;
 constexpr int kTileRows = VLJ_TILE_ROWS;
 constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block

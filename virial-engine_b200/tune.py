@@ -29,9 +29,10 @@ CANDIDATES = {
     "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
     "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
     "stream_c8": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8},
-    "stream_c16": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 16},
+    "ahead_c0": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 0},
+    "ahead_c4": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 4},
+    "ahead_c8": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 8},
     "tma_r1_s4": {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": 1, "VLJ_TILE_SLOTS": 4},
-    "tma_r4_s3": {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": 4, "VLJ_TILE_SLOTS": 3},
 }
 
 
