@@ -315,6 +315,45 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
     }
 
 
+def run_heat_flux(args, world, rank, stream):
+    """The large constant-energy box with the heat current sampled every step:
+    16,384,000 atoms (fcc 160^3 x 4, rho 0.8442), truncated-shifted, dt 0.004.
+    Its working set (15 GB) dwarfs the L2, so steps run back to back."""
+    import torch
+    import virial_lj as vl
+
+    p, box = vl.lattice_fcc(160, 0.8442, 0.722, 5 + rank)
+    n = len(p)
+    sim = vl.LennardJones(p, vl.Settings([box] * 3, cutoff=2.5, dt=0.004, skin=0.3),
+                          stream=stream.cuda_stream)
+    del p
+    steps = max(args.steps // 4, 10)
+    sim.record_heat_current(steps + 3)
+    for _ in range(3):
+        sim.step(1)
+        sim.sample_heat_current()
+    stream.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        sim.step(1)
+        sim.sample_heat_current()
+    e1.record(stream)
+    stream.synchronize()
+    ms = reduce_max(world, e0.elapsed_time(e1))
+    j = sim.read_heat_current()
+    m = sim.measure_now()
+    sim.close()
+    return {"workload": "lj-fcc160x4-16.4M-rho0.8442-truncated-nve-heat-current-every-step",
+            "value": world * n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "particles_per_box": n,
+            "config": {"dt": 0.004, "cutoff": 2.5, "skin": 0.3, "thermostat": "none",
+                       "sample": "one heat-current sample (3 x i64 fixed point) per step",
+                       "l2": "working set 15 GB, far above L2"},
+            "heat_current_samples": len(j), "list_overflow": m.list_overflow}
+
+
 def run_ours(args, world, rank, gpu_index):
     import numpy as np
     import torch
@@ -385,6 +424,7 @@ def run_ours(args, world, rank, gpu_index):
 
     # ---- the batched form on 512 uneven replicas, and the plain path on them ----
     batched = run_batched(args, world, rank, stream, flush_l2, peak, fp32_peak)
+    heat_flux = run_heat_flux(args, world, rank, stream)
     clk = clocks.stop() if rank == 0 else None
 
     # ---- end to end through the C ABI with host buffers ----
@@ -436,6 +476,7 @@ def run_ours(args, world, rank, gpu_index):
                               "peak_source": "measured live (FMA chains on every SM)"},
             "cpu_baseline": cpu,
             "batched": batched,
+            "heat_flux": heat_flux,
             "clocks": clk,
             "gpu_launches": launches,
             "list_rebuilds_timed": rebuilds,
