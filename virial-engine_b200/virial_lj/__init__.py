@@ -29,6 +29,7 @@ __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
     "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
+    "replica_cost", "shard_replicas",
 ]
 
 
@@ -608,3 +609,34 @@ def uneven_replicas(count=512, seed=2024, sizes=(500, 20000), densities=(0.01, 0
         p = lattice(n, side, t, seed + r)
         out.append(Replica(p, [side] * 3, Langevin(t, friction, (seed + r) & 0xFFFFFFFF)))
     return out
+
+
+def replica_cost(replica, cutoff=2.5, skin=0.3):
+    """Relative cost of stepping a replica: its particles times (the 96 B of
+    state each moves per step, plus its pair work at the machine balance of
+    about 11 flop per byte): 11 flops per list candidate and 20 per pair
+    inside the cutoff, at the replica's density."""
+    n = len(replica.particles)
+    volume = replica.box_size[0] * replica.box_size[1] * replica.box_size[2]
+    rho = n / volume
+    n_list = 4.0 / 3.0 * math.pi * (cutoff + skin) ** 3 * rho
+    n_rc = 4.0 / 3.0 * math.pi * cutoff ** 3 * rho
+    return n * (96.0 + (11.0 * n_list + 20.0 * n_rc) / 11.0)
+
+
+def shard_replicas(replicas, world_size, cutoff=2.5, skin=0.3):
+    """Whole replicas to ranks, balancing the summed cost (longest first, each
+    to the rank with the least so far). Returns one list of replica indices
+    per rank, each in ascending order; every rank computes the same answer."""
+    world_size = int(world_size)
+    if world_size < 1:
+        raise ValueError("world_size must be at least 1")
+    costs = [replica_cost(r, cutoff, skin) for r in replicas]
+    order = sorted(range(len(replicas)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world_size
+    shards = [[] for _ in range(world_size)]
+    for i in order:
+        rank = min(range(world_size), key=lambda k: (load[k], k))
+        shards[rank].append(i)
+        load[rank] += costs[i]
+    return [sorted(s) for s in shards]
