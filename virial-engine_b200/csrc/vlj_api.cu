@@ -870,6 +870,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));
     TRY(dalloc(s, &a.count, a.ncells));
     TRY(dalloc(s, &a.work, a.ncells));
+    TRY(dalloc(s, &a.rb_box, boxes.size()));
+    TRY(dalloc(s, &a.rb_first, boxes.size() + 1));
     TRY(dalloc(s, &a.list_count, seg));
     TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((cap + 3) / 4)));
     TRY(dalloc(s, &a.block_rows, ((size_t)seg + kForceThreads - 1) / kForceThreads));

@@ -76,9 +76,99 @@ __device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditiona
         }
     }
     __syncthreads();
+    if (a.nboxes == 1u) {
+        if (threadIdx.x == 0) {
+            const bool r = a.ctrl[0].rebuild != 0u;
+            a.rb_box[0] = 0u;
+            a.rb_first[0] = 0u;
+            a.rb_first[r ? 1 : 0] = r ? a.boxes[0].n : 0u;
+            g->rb_boxes = r ? 1u : 0u;
+            g->rb_slots = r ? a.boxes[0].n : 0u;
+            g->any = (uint32_t)s_any;
+            if (set) cudaGraphSetConditional(handle, (unsigned)s_any);
+        }
+        return;
+    }
+    // the rebuilding boxes, compacted in box order, with their particle counts
+    // summed before each: two block-wide exclusive scans per pass
+    __shared__ uint32_t s_wbox[32], s_wslot[32], s_cbox, s_cslot;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    if (threadIdx.x == 0) s_cbox = s_cslot = 0u;
+    __syncthreads();
+    for (uint32_t base = 0; base < a.nboxes; base += blockDim.x) {
+        const uint32_t b = base + threadIdx.x;
+        const bool flag = b < a.nboxes && a.ctrl[b].rebuild != 0u;
+        const uint32_t nb = flag ? a.boxes[b].n : 0u;
+        uint32_t ib = flag ? 1u : 0u, is = nb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t tb = __shfl_up_sync(0xffffffffu, ib, o);
+            const uint32_t ts = __shfl_up_sync(0xffffffffu, is, o);
+            if (lane >= (uint32_t)o) {
+                ib += tb;
+                is += ts;
+            }
+        }
+        if (lane == 31u) {
+            s_wbox[warp] = ib;
+            s_wslot[warp] = is;
+        }
+        __syncthreads();
+        uint32_t pb = s_cbox, ps = s_cslot;
+        for (uint32_t w = 0; w < warp; w++) {
+            pb += s_wbox[w];
+            ps += s_wslot[w];
+        }
+        if (flag) {
+            const uint32_t k = pb + ib - 1u;
+            a.rb_box[k] = b;
+            a.rb_first[k] = ps + is - nb;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (uint32_t w = 0; w < warps; w++) {
+                s_cbox += s_wbox[w];
+                s_cslot += s_wslot[w];
+            }
+        }
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
+        a.rb_first[s_cbox] = s_cslot;
+        g->rb_boxes = s_cbox;
+        g->rb_slots = s_cslot;
         g->any = (uint32_t)s_any;
         if (set) cudaGraphSetConditional(handle, (unsigned)s_any);
+    }
+}
+
+// Runs body(slot, box) for every particle of the boxes that rebuild this step
+// (Global::rb_slots of them), over a resident grid: each block takes 256
+// consecutive particles of the compacted list at a time, finds the first one's
+// box by bisection, and its threads step on from there. Every thread of the
+// block must call this.
+template <class F>
+__device__ __forceinline__ void for_rebuild_slots(const Arena& a, F body) {
+    __shared__ uint32_t s_k0;
+    const uint32_t total = a.glob->rb_slots, boxes = a.glob->rb_boxes;
+    for (uint32_t start = blockIdx.x * blockDim.x; start < total; start += gridDim.x * blockDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t lo = 0, hi = boxes;  // last k with rb_first[k] <= start
+            while (hi - lo > 1u) {
+                const uint32_t m = (lo + hi) >> 1;
+                if (a.rb_first[m] <= start) lo = m; else hi = m;
+            }
+            s_k0 = lo;
+        }
+        __syncthreads();
+        const uint32_t t = start + threadIdx.x;
+        if (t < total) {
+            uint32_t k = s_k0;
+            while (a.rb_first[k + 1] <= t) k++;
+            const uint32_t b = a.rb_box[k];
+            body(a.boxes[b].first + (t - a.rb_first[k]), b);
+        }
+        __syncthreads();
     }
 }
 

@@ -99,28 +99,26 @@ __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
 __global__ void bin_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
-    uint32_t b = box_of_slot(a, i);
-    if (!rebuilding(a, b)) return;
-    const Box& bx = a.boxes[b];
-    int32_t c[3];
+    for_rebuild_slots(a, [&](uint32_t i, uint32_t b) {
+        const Box& bx = a.boxes[b];
+        int32_t c[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        float hi = (float)a.x[k * a.seg + i];
-        int32_t v = (int32_t)floorf(__fdiv_rn(hi, bx.cell_size_f[k]));
-        int32_t m = (int32_t)bx.cells[k] - 1;
-        c[k] = v < 0 ? 0 : (v > m ? m : v);
-    }
-    uint32_t cell =
-        bx.cell_base + ((uint32_t)c[2] * bx.cells[1] + (uint32_t)c[1]) * bx.cells[0] + (uint32_t)c[0];
-    a.cell_of_slot[i] = cell;
-    atomicAdd(&a.count[cell], 1u);
-    // a force block wholly inside this box restarts its staged-row count
-    if (i % kForceThreads == 0u) {
-        const uint32_t end = min(i + (uint32_t)kForceThreads, a.nslots);
-        if (i >= bx.first && end <= bx.first + bx.n) a.block_rows[i / kForceThreads] = 0u;
-    }
+        for (int k = 0; k < 3; k++) {
+            float hi = (float)a.x[k * a.seg + i];
+            int32_t v = (int32_t)floorf(__fdiv_rn(hi, bx.cell_size_f[k]));
+            int32_t m = (int32_t)bx.cells[k] - 1;
+            c[k] = v < 0 ? 0 : (v > m ? m : v);
+        }
+        uint32_t cell = bx.cell_base +
+            ((uint32_t)c[2] * bx.cells[1] + (uint32_t)c[1]) * bx.cells[0] + (uint32_t)c[0];
+        a.cell_of_slot[i] = cell;
+        atomicAdd(&a.count[cell], 1u);
+        // a force block wholly inside this box restarts its staged-row count
+        if (i % kForceThreads == 0u) {
+            const uint32_t end = min(i + (uint32_t)kForceThreads, a.nslots);
+            if (i >= bx.first && end <= bx.first + bx.n) a.block_rows[i / kForceThreads] = 0u;
+        }
+    });
 }
 
 // ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
@@ -206,11 +204,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
 __global__ void scatter_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
-    if (!rebuilding(a, box_of_slot(a, i))) return;
-    uint32_t c = a.cell_of_slot[i];
-    a.sorted[a.cell_start[c] + atomicAdd(&a.count[c], 1u)] = i;
+    for_rebuild_slots(a, [&](uint32_t i, uint32_t) {
+        const uint32_t c = a.cell_of_slot[i];
+        a.sorted[a.cell_start[c] + atomicAdd(&a.count[c], 1u)] = i;
+    });
 }
 
 // ---- per-cell order (grid.wgsl:129-148) ----
@@ -292,27 +289,26 @@ __global__ void sort_kernel(Arena a) {
 __global__ void reorder_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nslots) return;
-    uint32_t b = box_of_slot(a, s);
-    if (!rebuilding(a, b) || !a.ctrl[b].reorder) return;
-    const Box& bx = a.boxes[b];
-    uint4 w;
-    double xs[3];
+    for_rebuild_slots(a, [&](uint32_t s, uint32_t b) {
+        if (!a.ctrl[b].reorder) return;
+        const Box& bx = a.boxes[b];
+        uint4 w;
+        double xs[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        xs[k] = a.sx[k * a.seg + s];
-        a.x[k * a.seg + s] = xs[k];
-        a.v[k * a.seg + s] = a.sv[k * a.seg + s];
-    }
-    a.id[s] = a.sid[s];
-    a.cell_of_slot[s] = a.scell[s];
-    a.sorted[s] = s;
-    w.x = encode(xs[0], bx.enc[0]);
-    w.y = encode(xs[1], bx.enc[1]);
-    w.z = encode(xs[2], bx.enc[2]);
-    w.w = 0u;
-    a.cache[a.glob->phase][s] = w;
+        for (int k = 0; k < 3; k++) {
+            xs[k] = a.sx[k * a.seg + s];
+            a.x[k * a.seg + s] = xs[k];
+            a.v[k * a.seg + s] = a.sv[k * a.seg + s];
+        }
+        a.id[s] = a.sid[s];
+        a.cell_of_slot[s] = a.scell[s];
+        a.sorted[s] = s;
+        w.x = encode(xs[0], bx.enc[0]);
+        w.y = encode(xs[1], bx.enc[1]);
+        w.z = encode(xs[2], bx.enc[2]);
+        w.w = 0u;
+        a.cache[a.glob->phase][s] = w;
+    });
 }
 
 // ---- the reference's packed positions for the list build
@@ -320,20 +316,19 @@ __global__ void reorder_kernel(Arena a) {
 __global__ void pack_kernel(Arena a) {
     count_kernel(a);
     if (!a.glob->any) return;
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nslots) return;
-    if (!rebuilding(a, box_of_slot(a, s))) return;
-    float h[3], l[3];
+    for_rebuild_slots(a, [&](uint32_t s, uint32_t) {
+        float h[3], l[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        double x = a.x[k * a.seg + s];
-        h[k] = (float)x;
-        l[k] = (float)(x - (double)h[k]);
-    }
-    float3 hi = make_float3(h[0], h[1], h[2]);
-    float3 lo = make_float3(l[0], l[1], l[2]);
-    a.ref[s] = make_float4(h[0], h[1], h[2], __uint_as_float(pack_lo(hi, lo)));
-    a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
+        for (int k = 0; k < 3; k++) {
+            double x = a.x[k * a.seg + s];
+            h[k] = (float)x;
+            l[k] = (float)(x - (double)h[k]);
+        }
+        float3 hi = make_float3(h[0], h[1], h[2]);
+        float3 lo = make_float3(l[0], l[1], l[2]);
+        a.ref[s] = make_float4(h[0], h[1], h[2], __uint_as_float(pack_lo(hi, lo)));
+        a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
+    });
 }
 
 // ---- launchers ----
@@ -361,7 +356,9 @@ cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long con
 }
 
 cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
-    const unsigned slots = blocks_for(a.nslots);
+    // the per-particle kernels cover the rebuilding boxes' particles from a
+    // resident grid
+    const unsigned slots = (unsigned)sm_count() * 8u;
     bin_kernel<<<slots, kBlock, 0, s>>>(a);
     scan_kernel<<<a.nboxes, kScanThreads, 0, s>>>(a);
     scatter_kernel<<<slots, kBlock, 0, s>>>(a);

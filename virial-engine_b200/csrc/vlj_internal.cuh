@@ -126,6 +126,8 @@ struct Global {
     uint32_t work_cells;         // entries of Arena::work this step
     uint32_t next_build;         // next work entry the list build takes
     uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
+    uint32_t rb_boxes;           // boxes that rebuild this step (Arena::rb_box)
+    uint32_t rb_slots;           // their particles, in all
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).
@@ -191,6 +193,11 @@ struct Arena {
     // the non-empty cells of the boxes that rebuild this step, in no set
     // order (the scan appends them; the sort and the list build take them)
     uint32_t* work;
+    // the boxes that rebuild this step (rb_boxes of them, ascending) and the
+    // running count of their particles before each (rb_first[rb_boxes] =
+    // rb_slots): the per-particle rebuild kernels cover only these
+    uint32_t* rb_box;
+    uint32_t* rb_first;
     uint32_t* list_count;
     uint32_t* list;
     // per force block (kForceThreads slots): rows (four entries each) of the
