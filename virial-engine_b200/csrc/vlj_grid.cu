@@ -242,7 +242,18 @@ __global__ void sort_kernel(Arena a) {
         const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
         const uint32_t m = end - start;
         if (lane == 0) a.count[cell] = 0u;
-        if (m <= 32u * kSortRegs) {
+        if (m <= 32u) {
+            // the usual cell: one key per lane, ranked against the m keys
+            const uint32_t key = (uint32_t)lane < m ? a.sorted[start + lane] : 0xffffffffu;
+            uint32_t rank = 0;
+            for (uint32_t src = 0; src < m; src++)
+                rank += __shfl_sync(0xffffffffu, key, src) < key ? 1u : 0u;
+            __syncwarp();
+            if ((uint32_t)lane < m) {
+                a.sorted[start + rank] = key;
+                if (reorder) move_to_scratch(a, key, start + rank, cell);
+            }
+        } else if (m <= 32u * kSortRegs) {
             uint32_t key[kSortRegs], rank[kSortRegs];
 #pragma unroll
             for (int r = 0; r < kSortRegs; r++) {
