@@ -51,7 +51,8 @@ ALGO_BYTES = 96          # f64 x and v read + written per particle-step
 
 
 BATCH = dict(replicas=512, seed=2024, sizes=(500, 20000), densities=(0.01, 0.90),
-             temperatures=(0.7, 2.0), friction=1.0, dt=0.004, cutoff=2.5, skin=0.3)
+             temperatures=(0.7, 2.0), friction=1.0, dt=0.004, cutoff=2.5, skin=0.3,
+             skins=(0.3, 0.4, 0.5, 0.6, 0.8))
 PLAIN_SAMPLE_EVERY = 16  # plain-path comparison: every 16th replica as its own simulation
 PLAIN_SAMPLE_STEPS = 50
 
@@ -226,7 +227,10 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
     reps = vl.uneven_replicas(BATCH["replicas"], BATCH["seed"] + 7919 * rank, BATCH["sizes"],
                               BATCH["densities"], BATCH["temperatures"], BATCH["friction"])
     total = sum(len(r.particles) for r in reps)
-    b = vl.Batch(reps, cutoff=BATCH["cutoff"], skin=BATCH["skin"], dt=BATCH["dt"],
+    # the neighbour skin for this set, chosen by the autotuner on this GPU
+    skin, skin_times = vl.tune_batch_skin(reps, BATCH["skins"], cutoff=BATCH["cutoff"],
+                                          dt=BATCH["dt"], stream=stream)
+    b = vl.Batch(reps, cutoff=BATCH["cutoff"], skin=skin, dt=BATCH["dt"],
                  stream=stream.cuda_stream)
     b.step(max(args.warmup, 3))
     stream.synchronize()
@@ -258,7 +262,7 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
     b.close()
     # rooflines with each replica's own density (truncated-shifted pairs)
     dens = [len(r.particles) / (r.box_size[0] * r.box_size[1] * r.box_size[2]) for r in reps]
-    flops = sum(len(r.particles) * flops_per_particle_step(d, 20.0, BATCH["cutoff"], BATCH["skin"])
+    flops = sum(len(r.particles) * flops_per_particle_step(d, 20.0, BATCH["cutoff"], skin)
                 for r, d in zip(reps, dens))
     bytes_ = ALGO_BYTES * total
     bound_s = max(bytes_ / (hbm_peak * 1e9), flops / (fp32_peak * 1e12)) if fp32_peak else None
@@ -293,7 +297,9 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
         "config": {"sizes": "N log-uniform in [500, 20000]", "densities": "uniform in [0.01, 0.90]",
                    "temperatures": "uniform in [0.7, 2.0], Langevin gamma=1.0",
                    "cutoff": BATCH["cutoff"], "cutoff_style": "truncated-shifted",
-                   "skin": BATCH["skin"], "dt": BATCH["dt"],
+                   "skin": skin, "skin_tuned_ms_per_step": {str(k): v * 1e3 for k, v in
+                                                             skin_times.items()},
+                   "plain_skin": BATCH["skin"], "dt": BATCH["dt"],
                    "seed": BATCH["seed"] + 7919 * rank,
                    "l2": "flushed between timed steps (256 MiB write on the stream)"},
         "gpu_launches": launches,

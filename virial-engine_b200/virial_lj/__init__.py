@@ -29,7 +29,7 @@ __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
     "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
-    "replica_cost", "shard_replicas",
+    "replica_cost", "shard_replicas", "tune_batch_skin",
 ]
 
 
@@ -640,3 +640,33 @@ def shard_replicas(replicas, world_size, cutoff=2.5, skin=0.3):
         shards[rank].append(i)
         load[rank] += costs[i]
     return [sorted(s) for s in shards]
+
+
+def tune_batch_skin(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), cutoff=2.5, dt=0.005,
+                    shifted_force=False, steps=60, warmup=20, stream=None):
+    """The neighbour skin that steps this replica set fastest on this GPU.
+
+    A wider skin makes longer lists (more work every step) but rebuilds them
+    less often; the best trade depends on the replicas' densities and
+    temperatures, so each candidate runs `warmup` then `steps` steps of the
+    actual set (timed with CUDA events through `torch.cuda`, on `stream`, a
+    torch stream). Forces are exact within the cutoff at any skin, so the choice
+    changes speed, not physics. Returns (best skin, {skin: seconds per step}).
+    """
+    import torch
+
+    s = stream or torch.cuda.current_stream()
+    times = {}
+    for skin in skins:
+        b = Batch(replicas, cutoff=cutoff, skin=skin, dt=dt, shifted_force=shifted_force,
+                  stream=s.cuda_stream)
+        b.step(warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        b.step(steps)
+        e1.record(s)
+        s.synchronize()
+        times[skin] = e0.elapsed_time(e1) / 1e3 / steps
+        b.close()
+    best = min(times, key=times.get)
+    return best, times
