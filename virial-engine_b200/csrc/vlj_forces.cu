@@ -283,10 +283,13 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
 __device__ __forceinline__ void langevin_noise(uint32_t id, unsigned long long step,
                                                uint32_t seed, float xi[3]) {
     const uint4 r = philox(id, step, seed);
-    const float u0 = __fdiv_rn((float)(r.x >> 8) + 1.0f, 16777216.0f);
-    const float u1 = __fdiv_rn((float)(r.y >> 8) + 1.0f, 16777216.0f);
-    const float u2 = __fdiv_rn((float)(r.z >> 8) + 1.0f, 16777216.0f);
-    const float u3 = __fdiv_rn((float)(r.w >> 8) + 1.0f, 16777216.0f);
+    // (q + 1) / 2^24 for a 24-bit q: the sum is exact and so is scaling by a
+    // power of two, so the product is the IEEE quotient
+    const float scale = 5.9604644775390625e-08f;  // 2^-24
+    const float u0 = ((float)(r.x >> 8) + 1.0f) * scale;
+    const float u1 = ((float)(r.y >> 8) + 1.0f) * scale;
+    const float u2 = ((float)(r.z >> 8) + 1.0f) * scale;
+    const float u3 = ((float)(r.w >> 8) + 1.0f) * scale;
     const float ra = sqrtf(-2.0f * logf(u0));
     const float aa = 6.283185307179586f * u1;
     const float rb = sqrtf(-2.0f * logf(u2));
