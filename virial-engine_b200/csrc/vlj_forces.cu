@@ -148,6 +148,8 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     const uint32_t my_rows = (cnt + 3u) / 4u;
     const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2], rc2 = bx.rc2;
     const float fshift = bx.force_shift;
+    // 0 < r2 < rc2 as one unsigned comparison of the bit patterns (r2 >= +0)
+    const uint32_t rc2_bits_m1 = __float_as_uint(rc2) - 1u;
     // The list's last row is padded with the particle itself, whose zero
     // separation drops out here with the entries beyond the cutoff.
     auto accumulate = [&](const uint4 pj) {
@@ -155,7 +157,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         const float dy = decode_diff(pj.y, own.y, dec1);
         const float dz = decode_diff(pj.z, own.z, dec2);
         const float r2 = dx * dx + dy * dy + dz * dz;
-        const bool in = r2 < rc2 && r2 > 0.0f;
+        const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
         // branch-free: most list entries are inside the cutoff; the select
         // drops whatever the pair math gives for entries that are not
         const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
