@@ -17,9 +17,10 @@ runs its own independent box (weak scaling, no collective on the step path);
 the time is the max over ranks.
 
 `e2e`: the same metric through the public API with host buffers: per bench
-step, the particles are written from host memory (vlj_write_particles),
+step, the particles are written from pinned host memory (vlj_write_particles),
 100 MD steps run (vlj_run), and the measurement and the particles are read
-back (vlj_measure_now, vlj_read_particles); wall clock, max over ranks.
+back into pinned host memory (vlj_measure_now, vlj_read_particles); wall
+clock, max over ranks.
 
 `--impl reference`: the reference has no CPU Lennard-Jones code and its GPU
 path needs a graphics API, so the reference arm is the CPU oracle's f64
@@ -433,9 +434,14 @@ def run_ours(args, world, rank, gpu_index):
     heat_flux = run_heat_flux(args, world, rank, stream)
     clk = clocks.stop() if rank == 0 else None
 
-    # ---- end to end through the C ABI with host buffers ----
+    # ---- end to end through the C ABI with host buffers (pinned) ----
     e2e_steps = max(3, min(args.steps, 10))
-    host = vl.lattice_fcc(WORK["cells"], WORK["density"], WORK["temperature"], WORK["seed"] + rank)[0]
+    start = vl.lattice_fcc(WORK["cells"], WORK["density"], WORK["temperature"], WORK["seed"] + rank)[0]
+    pinned_in = torch.empty(start.nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned_out = torch.empty(start.nbytes, dtype=torch.uint8, pin_memory=True)
+    host = pinned_in.numpy().view(vl.PARTICLE)
+    back = pinned_out.numpy().view(vl.PARTICLE)
+    host[:] = start
     sim.write_particles(host)
     sim.run(E2E_INNER)  # warm
     barrier(world)
@@ -444,7 +450,7 @@ def run_ours(args, world, rank, gpu_index):
         sim.write_particles(host)
         sim.run(E2E_INNER)
         meas = sim.measure_now()
-        back = sim.read_particles()
+        sim.read_particles(out=back)
     e2e_s = time.perf_counter() - t0
     e2e_max = reduce_max(world, e2e_s)
     e2e_value = world * n * E2E_INNER * e2e_steps / e2e_max
@@ -469,8 +475,9 @@ def run_ours(args, world, rank, gpu_index):
             "data": "synthetic", "config": config(n, world),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "note": f"per bench step: write particles, {E2E_INNER} MD steps, "
-                            "measure_now, read_particles; wall clock"},
+                    "note": f"per bench step: write particles from pinned host memory, "
+                            f"{E2E_INNER} MD steps, measure_now, read_particles into pinned "
+                            "host memory; wall clock"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "step_kernel<true>", "peak_source": peak_kind,

@@ -343,8 +343,14 @@ class LennardJones:
         return Measurement._from(m)
 
     # state
-    def read_particles(self):
-        out = np.zeros(self._n, PARTICLE)
+    def read_particles(self, out=None):
+        """Positions and canonical velocities in input order; into `out` (a
+        contiguous PARTICLE array of count() entries, e.g. over pinned host
+        memory) when given."""
+        if out is None:
+            out = np.zeros(self._n, PARTICLE)
+        elif out.dtype != PARTICLE or len(out) != self._n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous PARTICLE array of count() entries")
         _check(_lib.vlj_read_particles(self._h, _ffi.ptr(out)))
         return out
 
