@@ -5,7 +5,8 @@
 //   x, v      f64, structure of arrays: x[k * seg + slot], k = 0, 1, 2.
 //             v is stored half a kick behind (see the step kernel), so one
 //             force pass serves the closing half kick of a step and the
-//             opening half kick of the next.
+//             opening half kick of the next; with Nose-Hoover or the heat
+//             exchange it is canonical and the last forces are kept in acc.
 //   cache[2]  uint4 per slot: the position as 32-bit fractions of the box
 //             (X = round(x / L * 2^32) mod 2^32). Two copies: the step kernel
 //             reads one and writes the other; `phase` says which is current.
@@ -19,14 +20,17 @@
 //             The list build uses exactly the reference's f32 predicate on
 //             these, so lists match it bit for bit.
 //   list      u32 slot indices, interleaved by four: entry k of slot i at
-//             list[((k / 4) * seg + i) * 4 + k % 4], counts in list_count[i].
-//             A row of the list (four entries of every slot) is 16 B per
-//             slot, so the four lanes that serve a particle read one 16 B
-//             word and a warp reads one contiguous 128 B line; the force
-//             kernels stage row tiles into shared memory with TMA.
+//             list[((k / 4) * seg + i) * 4 + k % 4], counts in list_count[i];
+//             the last row's unused places hold i itself. A row of the list
+//             (four entries of one slot) is 16 B, so a thread reads a row with
+//             one load and a warp reads 512 contiguous bytes; the force
+//             kernels stream rows per thread past L1 (or, as a tuning option,
+//             stage row tiles into shared memory with TMA).
 //   cells     per cell: count (atomic cursor) and start. Boxes own contiguous
 //             runs of slots and cells, so one start array of ncells + 1 entries
 //             serves every box: box b's last cell ends where box b + 1 begins.
+//   work      per step, the non-empty cells of the rebuilding boxes; rb_box /
+//             rb_first the rebuilding boxes and their particle offsets.
 #pragma once
 
 #include <cuda.h>
@@ -37,11 +41,11 @@ namespace vlj {
 
 constexpr int kBlock = 256;
 constexpr int kSlots = 8;  // measurement accumulators per box
-// Force kernels: one thread per particle, kForceThreads per block; each TMA
-// tile holds kTileRows list rows (4 entries each) of the block's particles.
-// The tile ring's shared memory comes out of the same 256 KB per SM as the L1
-// that serves the neighbour gathers, so its depth is a tuning knob
-// (build.py --tune sweeps it).
+// Force kernels: one thread per particle, kForceThreads per block. With the
+// TMA tile ring (VLJ_LIST_STREAM=0) each tile holds kTileRows list rows (4
+// entries each) of the block's particles; the ring's shared memory comes out
+// of the same 256 KB per SM as the L1 that serves the neighbour gathers, so
+// its depth is a tuning knob (tune.py sweeps it).
 #ifndef VLJ_TILE_ROWS
 #define VLJ_TILE_ROWS 4
 #endif
