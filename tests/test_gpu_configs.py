@@ -1,0 +1,67 @@
+"""The remaining workload configurations as parity cases on the CUDA path.
+
+- 500 atoms on an fcc lattice (5^3 x 4) at rho 0.8442: the box (8.40) is under
+  three (cutoff + skin) wide, which the single-box path refuses as the
+  reference does, so it runs as a batch of one (two cells per axis, each
+  neighbour cell visited once); a short constant-energy trajectory against the
+  oracle's f64 engine (all pairs at this size) and its energy drift.
+- The liquid-vapour slab: 16,000 atoms on lattice_box(16000, [20, 20, 54.8])
+  lifted 47.6 into a 20 x 20 x 150 box, Langevin T = 0.7, gamma = 0.5,
+  force-shifted, dt 0.005, 300 profile bins: the slab keeps two interfaces,
+  the profiles add up to the whole box.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fcc500_small_box_as_a_batch_of_one(gpu, O):
+    p, L = gpu.lattice_fcc(5, 0.8442, 0.72, 1)
+    assert len(p) == 500 and L < 3 * 2.8
+    b = gpu.Batch([gpu.Replica(p, [L] * 3)], cutoff=2.5, skin=0.3, dt=0.005)
+    box = b.box_size(0)
+    md = O.MD(p["pos"], p["vel"], box, dt=0.005)
+    e0g = b.measure()[0].energy()
+    m0 = md.measure()
+    e0c = m0.kinetic + m0.potential
+    assert abs((e0g - e0c) / e0c) < 1e-6
+    b.run(20)
+    md.run(20)
+    q = b.read_particles(0)
+    pos, vel = md.read()
+    d = q["pos"] - pos
+    d -= np.array(box) * np.round(d / np.array(box))
+    assert np.abs(d).max() < 1e-5
+    assert np.abs(q["vel"] - vel).max() < 1e-4
+    b.run(980)
+    md.run(980)
+    m1 = md.measure()
+    dg = (b.measure()[0].energy() - e0g) / abs(e0g)
+    dc = (m1.kinetic + m1.potential - e0c) / abs(e0c)
+    assert abs(dg) <= 2.0 * abs(dc) + 2e-5, (dg, dc)
+
+
+@pytest.mark.slow
+def test_liquid_vapour_slab(gpu):
+    size = [20.0, 20.0, 150.0]
+    p = gpu.lattice_box(16_000, [20.0, 20.0, 54.8], 0.7, 3)
+    p["pos"][:, 2] += 47.6
+    sim = gpu.LennardJones(p, gpu.Settings(size, cutoff=2.5, dt=0.005, skin=0.3,
+                                           shifted_force=True, profile_bins=300,
+                                           thermostat=gpu.Langevin(0.7, 0.5, 11)))
+    sim.run(10_000)
+    sim.clear_profile()
+    for _ in range(200):
+        sim.step(20)
+        sim.sample_profile()
+    prof = sim.read_profile()
+    m = sim.measure_now()
+    assert len(prof.interfaces(0.37)) == 2
+    density = np.array(prof.density())
+    assert density.max() > 0.6 and density.min() < 0.05
+    assert abs(sum(s.particles for s in prof.slabs) - 16_000) < 1e-6
+    t = sum(sum(s.kinetic) for s in prof.slabs) / (3 * 16_000)
+    assert abs(t - 0.7) < 0.02
+    assert m.list_overflow == 0
