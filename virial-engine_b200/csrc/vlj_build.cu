@@ -14,13 +14,12 @@
 // the cells' candidates one stream in stencil order; it fetches the stream
 // kRound candidates at a time (slot, then encoded position, all loads of a
 // round in flight together) and copies those within reach of the home cell
-// into shared memory (a dense cell's all of them). A cell of kLaneHomes or
-// more particles then gives each lane a home particle to test against every
-// staged candidate in stream order; a sparser cell (dilute boxes) takes its
-// home particles in turn, the 32 lanes testing 32 staged candidates at once
-// and a ballot placing the accepted ones in the list in stream order. Either
-// way the inner loop reads only shared memory, and a dense home cell costs a
-// few rounds of two dependent loads.
+// into shared memory (a dense cell's all of them). The test then takes 32
+// staged candidates at a time, a lane each, against every home particle in
+// turn, so every lane is busy whatever the cell's occupancy; ballots hand each
+// home particle's lane its masks of accepted candidates, and the lane appends
+// them in stream order. The inner loops read only shared memory, and a dense
+// home cell costs a few rounds of two dependent loads.
 //
 // A test on the 32-bit encoded positions settles every candidate farther than
 // sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in); the two radii
@@ -37,7 +36,6 @@ namespace vlj {
 constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
 constexpr int kRound = 128;     // candidates a warp fetches per round
 constexpr int kStage = 512;     // staged candidates a warp holds (a dense cell's all)
-constexpr int kLaneHomes = 12;  // home particles from which a lane takes one each
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
 #endif
@@ -80,6 +78,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     // staged candidates: (x, y, z) as f32 offsets from the home cell's centre
     // (wide boxes) or as encoded words (narrow ones), the slot in w
     __shared__ uint4 s_cand[kBuildWarps][kStage];
+    __shared__ uint4 s_home[kBuildWarps][32];
     for (int t = threadIdx.x; t < 512; t += blockDim.x)
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
     __syncthreads();
@@ -171,10 +170,25 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
             uint32_t found = 0;  // this lane's home particle's list length so far
             const uint32_t homes = min(hend - h0, 32u);
             uint32_t staged = 0;
-            // where a full cell's lane writes its next entry: the row, and the
-            // place in it (entry `found`, kept while found < cap)
+            // where the lane writes its home particle's next entry: the row,
+            // and the place in it (entry `found`, kept while found < cap)
             uint32_t* wrow = a.list + (size_t)i * 4u;
             uint32_t wcol = 0;
+            auto append = [&](uint32_t j) {
+                if (found < cap) wrow[wcol] = j;
+                found += 1;
+                if (++wcol == 4u) {
+                    wcol = 0;
+                    wrow += row_stride;
+                }
+            };
+            // the home particles, for broadcast reads: f32 offsets from the
+            // cell's centre (wide boxes) or encoded words, slot in w
+            s_home[warp][lane] = wide ? make_uint4(__float_as_uint(own_rel[0]),
+                                                   __float_as_uint(own_rel[1]),
+                                                   __float_as_uint(own_rel[2]), i)
+                                      : make_uint4(own_enc.x, own_enc.y, own_enc.z, i);
+            __syncwarp();
             for (uint32_t base = 0; base < total; base += kRound) {
                 // Fetch the next kRound candidates of the stream (kRound / 32 per
                 // lane, loads in flight together), keep those within reach of the
@@ -235,87 +249,54 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 // another round
                 if (base + kRound < total && staged + kRound <= (uint32_t)kStage) continue;
                 __syncwarp();
-                // Squared separation of staged candidate e from a home
-                // particle at offsets (ox, oy, oz) / encoded words oe.
-                auto sep2 = [&](const uint4& e, float ox, float oy, float oz, const uint4& oe) {
+                // Test: 32 staged candidates at a time, a lane each, against
+                // every home particle in turn. Two ballots per home particle
+                // (near: inside the prefilter radius; sure: inside the accept
+                // radius) land in that particle's lane as 32-bit masks, so the
+                // test keeps every lane busy and the appends come after.
+                for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
+                    const uint32_t q = c0 + lane;
+                    const bool valid = q < staged;
+                    const uint4 e = s_cand[warp][valid ? q : 0u];
+                    unsigned my_sure = 0u, my_near = 0u;
                     if (wide) {
-                        const float dx = __uint_as_float(e.x) - ox;
-                        const float dy = __uint_as_float(e.y) - oy;
-                        const float dz = __uint_as_float(e.z) - oz;
-                        return dx * dx + dy * dy + dz * dz;
-                    }
-                    return encoded_r2(e, oe, dec);
-                };
-                if (homes >= (uint32_t)kLaneHomes) {
-                    // Full cells: each lane tests its home particle against
-                    // every staged candidate in stream order (one broadcast
-                    // shared-memory read per candidate for the whole warp).
-                    // The common outcomes -- out, or in by the encoded test --
-                    // take a few instructions; the reference's own arithmetic
-                    // runs only in the thin shell.
-                    auto append = [&](uint32_t j) {
-                        if (found < cap) wrow[wcol] = j;
-                        found += 1;
-                        if (++wcol == 4u) {
-                            wcol = 0;
-                            wrow += row_stride;
-                        }
-                    };
-                    if (wide) {
-                        const float ox = own_rel[0], oy = own_rel[1], oz = own_rel[2];
-#pragma unroll 2
-                        for (uint32_t q = 0; q < staged; q++) {
-                            const uint4 e = s_cand[warp][q];
-                            const float dx = __uint_as_float(e.x) - ox;
-                            const float dy = __uint_as_float(e.y) - oy;
-                            const float dz = __uint_as_float(e.z) - oz;
+                        const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
+                                    ez = __uint_as_float(e.z);
+                        for (uint32_t h = 0; h < homes; h++) {
+                            const uint4 hp = s_home[warp][h];
+                            const float dx = ex - __uint_as_float(hp.x);
+                            const float dy = ey - __uint_as_float(hp.y);
+                            const float dz = ez - __uint_as_float(hp.z);
                             const float r2e = dx * dx + dy * dy + dz * dz;
-                            if (r2e < pre_r2 && e.w != i &&
-                                (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510)))
-                                append(e.w);
+                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
+                            const unsigned mn = __ballot_sync(0xffffffffu, near);
+                            const unsigned ms = __ballot_sync(0xffffffffu, near && r2e < acc_r2);
+                            if (lane == h) {
+                                my_near = mn;
+                                my_sure = ms;
+                            }
                         }
                     } else {
-                        for (uint32_t q = 0; q < staged; q++) {
-                            const uint4 e = s_cand[warp][q];
-                            const float r2e = encoded_r2(e, own_enc, dec);
-                            if (home && r2e < pre_r2 && e.w != i &&
-                                (r2e < acc_r2 || ref_test(a, bx, i, e.w, s_q510)))
-                                append(e.w);
+                        for (uint32_t h = 0; h < homes; h++) {
+                            const uint4 hp = s_home[warp][h];
+                            const float r2e = encoded_r2(e, hp, dec);
+                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
+                            const unsigned mn = __ballot_sync(0xffffffffu, near);
+                            const unsigned ms = __ballot_sync(0xffffffffu, near && r2e < acc_r2);
+                            if (lane == h) {
+                                my_near = mn;
+                                my_sure = ms;
+                            }
                         }
                     }
-                } else {
-                    // Sparse cells: each home particle in turn against 32
-                    // staged candidates at once (a lane each); a ballot puts
-                    // the accepted ones in the list in stream order.
-                    for (uint32_t h = 0; h < homes; h++) {
-                        const uint32_t ih = __shfl_sync(0xffffffffu, i, h);
-                        uint32_t fh = __shfl_sync(0xffffffffu, found, h);
-                        const float ox = __shfl_sync(0xffffffffu, own_rel[0], h);
-                        const float oy = __shfl_sync(0xffffffffu, own_rel[1], h);
-                        const float oz = __shfl_sync(0xffffffffu, own_rel[2], h);
-                        const uint4 oe = make_uint4(__shfl_sync(0xffffffffu, own_enc.x, h),
-                                                    __shfl_sync(0xffffffffu, own_enc.y, h),
-                                                    __shfl_sync(0xffffffffu, own_enc.z, h), 0u);
-                        uint32_t* row_of_ih = a.list + (size_t)ih * 4u;
-                        for (uint32_t q0 = 0; q0 < staged; q0 += 32) {
-                            const uint32_t q = q0 + lane;
-                            bool in = false;
-                            uint32_t jq = 0;
-                            if (q < staged) {
-                                const uint4 e = s_cand[warp][q];
-                                const float r2e = sep2(e, ox, oy, oz, oe);
-                                jq = e.w;
-                                if (r2e < pre_r2 && jq != ih)
-                                    in = r2e < acc_r2 || ref_test(a, bx, ih, jq, s_q510);
-                            }
-                            const unsigned acc = __ballot_sync(0xffffffffu, in);
-                            if (in) {
-                                const uint32_t k = fh + (uint32_t)__popc(acc & below);
-                                if (k < cap) row_of_ih[(size_t)(k >> 2) * row_stride + (k & 3u)] = jq;
-                            }
-                            fh += (uint32_t)__popc(acc);
-                        }
-                        if (lane == h) found = fh;
+                    // each home particle's lane appends its accepted candidates
+                    // in stream order; the thin shell takes the reference's test
+                    unsigned m = my_near;
+                    while (m) {
+                        const uint32_t bit = (uint32_t)__ffs(m) - 1u;
+                        m &= m - 1u;
+                        const uint32_t jq = s_cand[warp][c0 + bit].w;
+                        if (((my_sure >> bit) & 1u) || ref_test(a, bx, i, jq, s_q510)) append(jq);
                     }
                 }
                 __syncwarp();
