@@ -86,7 +86,6 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     // Warps take home cells from the step's work list (the non-empty cells of
     // the boxes that rebuild) until it runs out.
     const uint32_t cells = a.glob->work_cells;
-    uint32_t longest = 0;
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(&a.glob->next_build, 1u);
@@ -313,19 +312,18 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 a.list_count[i] = kept;
                 if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
                 a.snap[i] = own_enc;
-                longest = max(longest, kept);
             }
-            // rows each force block stages: one atomic per block these lanes
-            // touch (a cell's slots are mostly in one block after a reorder)
+#if !VLJ_LIST_STREAM
+            // rows each force block stages in its TMA tiles: one atomic per
+            // block these lanes touch (a cell's slots are mostly in one block
+            // after a reorder)
             const uint32_t blk = home ? i / (uint32_t)kForceThreads : 0xffffffffu;
             const unsigned peers = __match_any_sync(0xffffffffu, blk);
             const uint32_t rows = __reduce_max_sync(peers, home ? (kept + 3u) / 4u : 0u);
             if (home && lane == (uint32_t)(__ffs(peers) - 1)) atomicMax(&a.block_rows[blk], rows);
+#endif
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
-    if (lane == 0 && longest) atomicMax(&a.glob->max_count, longest);
 }
 
 cudaError_t launch_build_list(const Arena& a, cudaStream_t s) {

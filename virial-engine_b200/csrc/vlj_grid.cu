@@ -113,11 +113,13 @@ __global__ void bin_kernel(Arena a) {
             ((uint32_t)c[2] * bx.cells[1] + (uint32_t)c[1]) * bx.cells[0] + (uint32_t)c[0];
         a.cell_of_slot[i] = cell;
         atomicAdd(&a.count[cell], 1u);
+#if !VLJ_LIST_STREAM
         // a force block wholly inside this box restarts its staged-row count
         if (i % kForceThreads == 0u) {
             const uint32_t end = min(i + (uint32_t)kForceThreads, a.nslots);
             if (i >= bx.first && end <= bx.first + bx.n) a.block_rows[i / kForceThreads] = 0u;
         }
+#endif
     });
 }
 

@@ -126,7 +126,7 @@ struct Global {
     uint32_t fault;      // first error a kernel recorded (0 none)
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
-    uint32_t max_count;          // longest list built so far
+    uint32_t unused;
     uint32_t work_cells;         // entries of Arena::work this step
     uint32_t next_build;         // next work entry the list build takes
     uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
@@ -204,8 +204,9 @@ struct Arena {
     uint32_t* rb_first;
     uint32_t* list_count;
     uint32_t* list;
-    // per force block (kForceThreads slots): rows (four entries each) of the
-    // longest list in it, so a block stages only the rows its particles use. Reset at each rebuild of
+    // per force block (kForceThreads slots), for the TMA tile ring only: rows
+    // (four entries each) of the longest list in it, so a block stages only
+    // the rows its particles use. Reset at each rebuild of
     // the box that holds the whole block; a block across two boxes keeps the
     // largest value it ever had (more rows staged, never fewer).
     uint32_t* block_rows;
