@@ -316,7 +316,9 @@ vlj_status vlj_create(const vlj_particle* particles, size_t count, const vlj_set
     if (!out) return fail(VLJ_INVALID_ARG, "out is null");
     *out = nullptr;
     if (!particles || count == 0) return fail(VLJ_INVALID_ARG, "no particles");
-    if (count >= (1ull << 31)) return fail(VLJ_INVALID_ARG, "at most 2^31 - 1 particles");
+    // list offsets are 32-bit (a slot's four entries per row, rows 4 * seg
+    // apart); 2^30 particles' lists would be far beyond one GPU's memory anyway
+    if (count >= (1ull << 30)) return fail(VLJ_INVALID_ARG, "at most 2^30 - 1 particles");
     TRY(check_settings(settings));
     int devices = 0;
     vlj_device_count(&devices);
@@ -823,7 +825,7 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
         cells += b.total_cells;
         cap = std::max(cap, b.capacity);
     }
-    if (slots >= (1ull << 31)) return fail(VLJ_INVALID_ARG, "at most 2^31 - 1 particles in all");
+    if (slots >= (1ull << 30)) return fail(VLJ_INVALID_ARG, "at most 2^30 - 1 particles in all");
     if (cells >= (1ull << 32) - 1) return fail(VLJ_INVALID_ARG, "too many cells in all boxes");
     if (batched)
         s->replicas = boxes;

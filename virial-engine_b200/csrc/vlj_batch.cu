@@ -152,7 +152,7 @@ vlj_status vlj_batch_create(const vlj_replica_desc* replicas, size_t count, doub
             return fail(VLJ_NOT_ENABLED, "replicas take Langevin or no thermostat");
         total += replicas[r].count;
     }
-    if (total >= (1ull << 31)) return fail(VLJ_INVALID_ARG, "at most 2^31 - 1 particles in all");
+    if (total >= (1ull << 30)) return fail(VLJ_INVALID_ARG, "at most 2^30 - 1 particles in all");
     int devices = 0;
     vlj_device_count(&devices);
     if (devices == 0) return fail(VLJ_NO_DEVICE, "no CUDA device is visible");

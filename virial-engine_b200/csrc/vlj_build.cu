@@ -16,10 +16,11 @@
 // round in flight together) and copies those within reach of the home cell
 // into shared memory (a dense cell's all of them). The test then takes 32
 // staged candidates at a time, a lane each, against every home particle in
-// turn, so every lane is busy whatever the cell's occupancy; ballots hand each
-// home particle's lane its masks of accepted candidates, and the lane appends
-// them in stream order. The inner loops read only shared memory, and a dense
-// home cell costs a few rounds of two dependent loads.
+// turn, so every lane is busy whatever the cell's occupancy; the lanes that
+// accept write their candidates into that home particle's list at once (its
+// count so far plus their rank in the ballot, so stream order). The inner
+// loops read only shared memory, and a dense home cell costs a few rounds of
+// two dependent loads.
 //
 // A test on the 32-bit encoded positions settles every candidate farther than
 // sqrt(prefilter_r2) (out) or nearer than sqrt(accept_r2) (in); the two radii
@@ -61,6 +62,12 @@ __device__ __noinline__ bool ref_test(const Arena& a, const Box& bx, uint32_t i,
     const float r2 =
         __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2]));
     return r2 < bx.list_r2;
+}
+
+// A store the predicate guards, without a branch around it.
+__device__ __forceinline__ void store_if(bool p, uint32_t* ptr, uint32_t v) {
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %2, 0;\n @q st.global.u32 [%0], %1;\n}"
+                 ::"l"(ptr), "r"(v), "r"((uint32_t)p) : "memory");
 }
 
 // Whether stencil offset d (-1, 0, 1) along an axis of n cells reaches a cell
@@ -152,7 +159,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
         uint32_t mid[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) mid[k] = home_lo[k] + home_w[k] / 2u;
-        const size_t row_stride = (size_t)a.seg * 4u;
+        const uint32_t row_stride = a.seg * 4u;  // entries between a slot's rows
         const unsigned below = (1u << lane) - 1u;
         for (uint32_t h0 = hbeg; h0 < hend; h0 += 32) {
             const bool home = h0 + lane < hend;
@@ -166,21 +173,11 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 own_rel[1] = (float)(int32_t)(own_enc.y - mid[1]) * dec[1];
                 own_rel[2] = (float)(int32_t)(own_enc.z - mid[2]) * dec[2];
             }
-            uint32_t found = 0;  // this lane's home particle's list length so far
+            // this lane's home particle's list length so far (every accepted
+            // candidate, also those past the capacity)
+            uint32_t found = 0;
             const uint32_t homes = min(hend - h0, 32u);
             uint32_t staged = 0;
-            // where the lane writes its home particle's next entry: the row,
-            // and the place in it (entry `found`, kept while found < cap)
-            uint32_t* wrow = a.list + (size_t)i * 4u;
-            uint32_t wcol = 0;
-            auto append = [&](uint32_t j) {
-                if (found < cap) wrow[wcol] = j;
-                found += 1;
-                if (++wcol == 4u) {
-                    wcol = 0;
-                    wrow += row_stride;
-                }
-            };
             // the home particles, for broadcast reads: f32 offsets from the
             // cell's centre (wide boxes) or encoded words, slot in w
             s_home[warp][lane] = wide ? make_uint4(__float_as_uint(own_rel[0]),
@@ -249,15 +246,32 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 if (base + kRound < total && staged + kRound <= (uint32_t)kStage) continue;
                 __syncwarp();
                 // Test: 32 staged candidates at a time, a lane each, against
-                // every home particle in turn. Two ballots per home particle
-                // (near: inside the prefilter radius; sure: inside the accept
-                // radius) land in that particle's lane as 32-bit masks, so the
-                // test keeps every lane busy and the appends come after.
+                // every home particle in turn. The lanes that accept write
+                // their candidates into that home particle's list themselves,
+                // in stream order (its count so far plus the rank in the
+                // ballot), so every lane is busy whatever the cell's
+                // occupancy and however unevenly the homes accept. Candidates
+                // in the thin shell between the two radii take the
+                // reference's test.
                 for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
                     const uint32_t q = c0 + lane;
                     const bool valid = q < staged;
                     const uint4 e = s_cand[warp][valid ? q : 0u];
-                    unsigned my_sure = 0u, my_near = 0u;
+                    auto settle = [&](uint32_t h, uint32_t home_slot, float r2e) {
+                        const bool near = valid && r2e < pre_r2 && e.w != home_slot;
+                        bool take = near && r2e < acc_r2;
+                        if (near && !take) take = ref_test(a, bx, home_slot, e.w, s_q510);
+                        const unsigned m = __ballot_sync(0xffffffffu, take);
+                        if (m == 0u) return;
+                        const uint32_t k = __shfl_sync(0xffffffffu, found, h) +
+                                           (uint32_t)__popc(m & below);
+                        // entry k of the home particle's list: row k / 4, place k % 4
+                        store_if(take && k < cap,
+                                 a.list + ((unsigned long long)(k >> 2) * row_stride +
+                                           (home_slot * 4u + (k & 3u))),
+                                 e.w);
+                        if (lane == h) found += (uint32_t)__popc(m);
+                    };
                     if (wide) {
                         const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
                                     ez = __uint_as_float(e.z);
@@ -266,36 +280,13 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                             const float dx = ex - __uint_as_float(hp.x);
                             const float dy = ey - __uint_as_float(hp.y);
                             const float dz = ez - __uint_as_float(hp.z);
-                            const float r2e = dx * dx + dy * dy + dz * dz;
-                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
-                            const unsigned mn = __ballot_sync(0xffffffffu, near);
-                            const unsigned ms = __ballot_sync(0xffffffffu, near && r2e < acc_r2);
-                            if (lane == h) {
-                                my_near = mn;
-                                my_sure = ms;
-                            }
+                            settle(h, hp.w, dx * dx + dy * dy + dz * dz);
                         }
                     } else {
                         for (uint32_t h = 0; h < homes; h++) {
                             const uint4 hp = s_home[warp][h];
-                            const float r2e = encoded_r2(e, hp, dec);
-                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
-                            const unsigned mn = __ballot_sync(0xffffffffu, near);
-                            const unsigned ms = __ballot_sync(0xffffffffu, near && r2e < acc_r2);
-                            if (lane == h) {
-                                my_near = mn;
-                                my_sure = ms;
-                            }
+                            settle(h, hp.w, encoded_r2(e, hp, dec));
                         }
-                    }
-                    // each home particle's lane appends its accepted candidates
-                    // in stream order; the thin shell takes the reference's test
-                    unsigned m = my_near;
-                    while (m) {
-                        const uint32_t bit = (uint32_t)__ffs(m) - 1u;
-                        m &= m - 1u;
-                        const uint32_t jq = s_cand[warp][c0 + bit].w;
-                        if (((my_sure >> bit) & 1u) || ref_test(a, bx, i, jq, s_q510)) append(jq);
                     }
                 }
                 __syncwarp();

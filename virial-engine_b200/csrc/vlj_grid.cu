@@ -128,7 +128,7 @@ __global__ void bin_kernel(Arena a) {
 // The box's non-empty cells join the step's work list for the sort and the
 // list build.
 constexpr int kScanThreads = 1024;
-constexpr int kScanPer = 4;
+constexpr int kScanPer = 16;  // counts per thread: a box of up to 16,384 cells in one pass
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     count_kernel(a);

@@ -58,6 +58,11 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #ifndef VLJ_LIST_STREAM
 #define VLJ_LIST_STREAM 1
 #endif
+// 1: the pair force's reciprocal (square root) as the flush-to-zero PTX
+// approximation (rsqrt_pair / rcp_pair below); 0: rsqrtf / __fdividef.
+#ifndef VLJ_FTZ_PAIR
+#define VLJ_FTZ_PAIR 1
+#endif
 // 1: with streamed rows, issue the next row's neighbour gathers before
 // computing this row's pairs (twice the loads in flight, more registers).
 #ifndef VLJ_GATHER_AHEAD
@@ -325,18 +330,44 @@ __device__ __forceinline__ void lj_pair(float r2, const Box& b, float& rf, float
     }
 }
 
+// 1 / sqrt(x) and 1 / x as the PTX approximations rsqrtf and __fdividef(1, x)
+// use, in their flush-to-zero forms: the same values for normal inputs, without
+// the subnormal-range handling around the hardware instruction. A list entry's
+// r^2 is never subnormal: it is at least a few tenths (pairs closer than that
+// have energies far beyond any simulated state) or exactly 0 for the padding,
+// whose result the cutoff test drops either way.
+__device__ __forceinline__ float rsqrt_pair(float x) {
+#if VLJ_FTZ_PAIR
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+#else
+    return rsqrtf(x);
+#endif
+}
+
+__device__ __forceinline__ float rcp_pair(float x) {
+#if VLJ_FTZ_PAIR
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+#else
+    return __fdividef(1.0f, x);
+#endif
+}
+
 // |F| / r of a pair at r2 < rc2: the factor that multiplies the separation.
 template <bool SHIFTED_FORCE>
 __device__ __forceinline__ float lj_force_over_r2(float r2, float force_shift) {
     if (SHIFTED_FORCE) {
         // one reciprocal square root gives both 1/r^2 and r
-        const float inv_r = rsqrtf(r2);
+        const float inv_r = rsqrt_pair(r2);
         const float inv2 = inv_r * inv_r;
         const float s6 = inv2 * inv2 * inv2;
         const float rf = 24.0f * s6 * (2.0f * s6 - 1.0f) - r2 * inv_r * force_shift;
         return rf * inv2;
     }
-    const float inv2 = __fdividef(1.0f, r2);
+    const float inv2 = rcp_pair(r2);
     const float s6 = inv2 * inv2 * inv2;
     return 24.0f * s6 * (2.0f * s6 - 1.0f) * inv2;
 }
