@@ -145,12 +145,29 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     for (uint32_t tile = 0; tile < total; tile += kScanThreads * kScanPer) {
         uint32_t v[kScanPer];
         uint32_t sum = 0;
+        const uint32_t c_first = tile + threadIdx.x * kScanPer;
+        // a thread's counts as 16-byte loads where they are aligned and whole
+        // (a single box starts at cell 0)
+        const bool vec = (base & 3u) == 0u && c_first + kScanPer <= total;
+        if (vec) {
+            const uint4* p = reinterpret_cast<const uint4*>(a.count + base + c_first);
 #pragma unroll
-        for (int q = 0; q < kScanPer; q++) {
-            uint32_t c = tile + threadIdx.x * kScanPer + q;
-            v[q] = c < total ? a.count[base + c] : 0u;
-            sum += v[q];
+            for (int r = 0; r < kScanPer / 4; r++) {
+                const uint4 w = p[r];
+                v[4 * r] = w.x;
+                v[4 * r + 1] = w.y;
+                v[4 * r + 2] = w.z;
+                v[4 * r + 3] = w.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kScanPer; q++) {
+                const uint32_t c = c_first + q;
+                v[q] = c < total ? a.count[base + c] : 0u;
+            }
         }
+#pragma unroll
+        for (int q = 0; q < kScanPer; q++) sum += v[q];
         // inclusive scan of the per-thread sums
         uint32_t incl = sum;
 #pragma unroll
@@ -171,14 +188,30 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
         }
         __syncthreads();
         uint32_t before = s_carry + (warp ? s_warp[warp - 1] : 0u) + incl - sum;
+        if (vec) {
+            uint4* st = reinterpret_cast<uint4*>(a.cell_start + base + c_first);
+            uint4* zero = reinterpret_cast<uint4*>(a.count + base + c_first);
 #pragma unroll
-        for (int q = 0; q < kScanPer; q++) {
-            uint32_t c = tile + threadIdx.x * kScanPer + q;
-            if (c < total) {
-                a.cell_start[base + c] = before;
-                a.count[base + c] = 0u;
+            for (int r = 0; r < kScanPer / 4; r++) {
+                uint4 w;
+                w.x = before;
+                w.y = w.x + v[4 * r];
+                w.z = w.y + v[4 * r + 1];
+                w.w = w.z + v[4 * r + 2];
+                before = w.w + v[4 * r + 3];
+                st[r] = w;
+                zero[r] = make_uint4(0u, 0u, 0u, 0u);
             }
-            before += v[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < kScanPer; q++) {
+                const uint32_t c = c_first + q;
+                if (c < total) {
+                    a.cell_start[base + c] = before;
+                    a.count[base + c] = 0u;
+                }
+                before += v[q];
+            }
         }
         // append the non-empty cells to the work list: one atomic per warp
         uint32_t nz = 0;
