@@ -259,10 +259,13 @@ class LennardJones:
         _check(_lib.vlj_create(_ffi.ptr(p), len(p), C.byref(cs), stream, C.byref(h)))
         self._h = h
         self._n = len(p)
+        # kept on the object: a collection at interpreter exit may run after
+        # the module's globals are gone
+        self._destroy = _lib.vlj_destroy
 
     def close(self):
         if getattr(self, "_h", None):
-            _lib.vlj_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -500,10 +503,11 @@ class Batch:
         self._h = h
         self._counts = [len(p) for p in self._keep]
         self._keep = None
+        self._destroy = _lib.vlj_batch_destroy
 
     def close(self):
         if getattr(self, "_h", None):
-            _lib.vlj_batch_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):
