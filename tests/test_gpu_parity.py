@@ -259,5 +259,5 @@ def test_kernel_counter_counts_skipped_rebuilds_out(gpu):
     k1 = sim.kernels_executed()
     r1 = sim.measure_now().list_rebuilds
     # a step kernel per step, a decide per 16-step graph (the step kernels take
-    # the later steps' decisions), seven per rebuild
-    assert k1 - k0 == 64 + 64 // 16 + 7 * (r1 - r0)
+    # the later steps' decisions), six per rebuild
+    assert k1 - k0 == 64 + 64 // 16 + 6 * (r1 - r0)

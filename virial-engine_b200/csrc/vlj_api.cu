@@ -865,8 +865,6 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.cache[0], seg));
     TRY(dalloc(s, &a.cache[1], seg));
     TRY(dalloc(s, &a.snap, seg));
-    TRY(dalloc(s, &a.ref, seg));
-    TRY(dalloc(s, &a.ref_lo, seg));
     TRY(dalloc(s, &a.cell_of_slot, seg));
     TRY(dalloc(s, &a.sorted, seg));
     TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));

@@ -42,20 +42,33 @@ constexpr int kStage = 512;     // staged candidates a warp holds (a dense cell'
 #endif
 constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;  // register budget of the build
 
+// The reference's packed position of slot s: the f32 hi part of each f64
+// coordinate and the f32 lo part of the rest (Df64::from_f64,
+// lennard_jones.rs:476-489, lennard_jones.wgsl:154-164).
+__device__ __forceinline__ void ref_parts(const Arena& a, uint32_t s, float h[3], float l[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double x = a.x[(size_t)k * a.seg + s];
+        h[k] = (float)x;
+        l[k] = (float)(x - (double)h[k]);
+    }
+}
+
 // The reference's predicate for slots i and j: nearest((pj.hi - xh) +
 // (unpack(pj) - xl)), squared length < list_r2, in f32 as written
-// (lennard_jones.wgsl:482-484). Loads its operands itself: it runs only for
-// candidates in the thin shell around the list radius.
+// (lennard_jones.wgsl:482-484), where unpack(pj) is pj's lo part as the
+// reference packs it (nine bits of its hi part's last bit). Derives its
+// operands from the f64 positions itself: it runs only for candidates in the
+// thin shell around the list radius.
 __device__ __noinline__ bool ref_test(const Arena& a, const Box& bx, uint32_t i, uint32_t j,
                                       const float* q510) {
-    const float4 own = a.ref[i], own_lo = a.ref_lo[i], pj = a.ref[j];
-    const float xh[3] = {own.x, own.y, own.z}, xl[3] = {own_lo.x, own_lo.y, own_lo.z};
-    const float ph[3] = {pj.x, pj.y, pj.z};
-    const uint32_t bits = __float_as_uint(pj.w);
+    float xh[3], xl[3], ph[3], pl[3];
+    ref_parts(a, i, xh, xl);
+    ref_parts(a, j, ph, pl);
     float d[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        const float lo = __fmul_rn(q510[(bits >> (9u * k)) & 511u], last_bit(ph[k]));
+        const float lo = packed_lo(ph[k], pl[k], q510);
         const float e = __fadd_rn(__fsub_rn(ph[k], xh[k]), __fsub_rn(lo, xl[k]));
         d[k] = nearest_ref_fast(e, bx.box_f[k], bx.inv_box_f[k]);
     }

@@ -2,7 +2,7 @@
 //
 // A step starts with `decide` (one block: flip the position copy, pick the
 // boxes that rebuild). The rebuild chain that follows -- bin, scan, scatter,
-// per-cell order with the optional reorder, copy back, pack, list build --
+// per-cell order with the optional reorder, copy back, list build --
 // sits under a conditional graph node, so it runs only on steps where some
 // box crossed the skin / 2 trigger; launched directly, each kernel returns at
 // once when nothing rebuilds. Reference kernels are cited at each kernel.
@@ -357,26 +357,6 @@ __global__ void reorder_kernel(Arena a) {
     });
 }
 
-// ---- the reference's packed positions for the list build
-// (lennard_jones.wgsl:154-164; hi/lo as Df64::from_f64, lennard_jones.rs:476-489)
-__global__ void pack_kernel(Arena a) {
-    count_kernel(a);
-    if (!a.glob->any) return;
-    for_rebuild_slots(a, [&](uint32_t s, uint32_t) {
-        float h[3], l[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            double x = a.x[k * a.seg + s];
-            h[k] = (float)x;
-            l[k] = (float)(x - (double)h[k]);
-        }
-        float3 hi = make_float3(h[0], h[1], h[2]);
-        float3 lo = make_float3(l[0], l[1], l[2]);
-        a.ref[s] = make_float4(h[0], h[1], h[2], __uint_as_float(pack_lo(hi, lo)));
-        a.ref_lo[s] = make_float4(l[0], l[1], l[2], 0.0f);
-    });
-}
-
 // ---- launchers ----
 cudaError_t launch_encode(const Arena& a, cudaStream_t s) {
     encode_kernel<<<blocks_for(a.nslots), kBlock, 0, s>>>(a);
@@ -410,9 +390,8 @@ cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
     scatter_kernel<<<slots, kBlock, 0, s>>>(a);
     sort_kernel<<<(unsigned)sm_count() * 8u, kBlock, 0, s>>>(a);
     reorder_kernel<<<slots, kBlock, 0, s>>>(a);
-    pack_kernel<<<slots, kBlock, 0, s>>>(a);
     launch_build_list(a, s);  // vlj_build.cu
-    return after_launch(7);
+    return after_launch(6);
 }
 
 }  // namespace vlj

@@ -14,11 +14,10 @@
 //             minimum image for free, at 32-bit resolution on any box size.
 //   snap      uint4 per slot: the cache word at the last list build, for the
 //             skin / 2 displacement trigger.
-//   ref       float4 per slot, written at each rebuild: the reference's
-//             packed position (f32 hi in xyz, lo as three 9-bit fractions of
-//             the hi part's last bit in w) and ref_lo (the full f32 lo part).
-//             The list build uses exactly the reference's f32 predicate on
-//             these, so lists match it bit for bit.
+//   (no copy of the reference's packed positions is kept: the list build
+//   settles all but a thin shell of candidates on the 32-bit words and, for
+//   that shell, derives the reference's f32 hi / packed lo parts from x and
+//   applies the reference's f32 predicate, so lists match it bit for bit)
 //   list      u32 slot indices, interleaved by four: entry k of slot i at
 //             list[((k / 4) * seg + i) * 4 + k % 4], counts in list_count[i];
 //             the last row's unused places hold i itself. A row of the list
@@ -193,8 +192,6 @@ struct Arena {
     uint32_t* id;
     uint4* cache[2];
     uint4* snap;
-    float4* ref;
-    float4* ref_lo;
     uint32_t* cell_of_slot;
     uint32_t* sorted;
     uint32_t* cell_start;  // ncells + 1
@@ -267,23 +264,15 @@ __device__ __forceinline__ float last_bit(float h) {
     return __uint_as_float((e - 23u) << 23);
 }
 
-__device__ __forceinline__ uint32_t pack_lo(float3 hi, float3 lo) {
-    uint32_t bits = 0x20000000u;
-    float h[3] = {hi.x, hi.y, hi.z};
-    float l[3] = {lo.x, lo.y, lo.z};
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        float t = __fdiv_rn(l[k], last_bit(h[k]));
-        t = fminf(fmaxf(t, -0.5f), 0.5f);
-        int32_t q = (int32_t)rintf(__fmul_rn(t, 510.0f));
-        bits |= (uint32_t)(q + 256) << (9u * (uint32_t)k);
-    }
-    return bits;
-}
-
-__device__ __forceinline__ float unpack_lo1(float h, uint32_t bits, int k) {
-    float q = (float)((int32_t)((bits >> (9u * (uint32_t)k)) & 511u) - 256);
-    return __fmul_rn(__fdiv_rn(q, 510.0f), last_bit(h));
+// One axis of the reference's packed lo part: the f32 lo part as a 9-bit
+// fraction q / 510 of the hi part's last bit, and back (pack_lo / unpack_lo,
+// lennard_jones.wgsl:128-152). `q510` holds q / 510 for q = -256..255.
+__device__ __forceinline__ float packed_lo(float h, float l, const float* q510) {
+    const float unit = last_bit(h);
+    float t = __fdiv_rn(l, unit);
+    t = fminf(fmaxf(t, -0.5f), 0.5f);
+    const int32_t q = (int32_t)rintf(__fmul_rn(t, 510.0f));
+    return __fmul_rn(q510[q + 256], unit);
 }
 
 // nearest image, lennard_jones.wgsl:199-202
