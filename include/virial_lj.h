@@ -179,6 +179,12 @@ VLJ_API vlj_status vlj_set_temperature(vlj_sim *sim, double temperature);
 VLJ_API vlj_status vlj_set_heat_exchange(vlj_sim *sim, const vlj_heat_exchange *exchange);
 /* *has = 0 when no exchange is set. */
 VLJ_API vlj_status vlj_heat_flux(const vlj_sim *sim, int *has, double *flux);
+/* No reference counterpart (the reference bins only when the lists rebuild):
+ * with on != 0, rebuild the cell grid (bin, scan, scatter, per-cell sort) on
+ * every step, the Verlet lists still on the skin / 2 trigger. Same trajectory
+ * to the bit, more work per step. A single box only (VLJ_NOT_ENABLED for a
+ * batch's simulation). */
+VLJ_API vlj_status vlj_set_grid_every_step(vlj_sim *sim, int on);
 
 /* ---- profiles along z: sample_profile / clear_profile / read_profile
  * (lennard_jones.rs:1167-1191, 1286-1325). `slabs` holds profile_bins

@@ -266,6 +266,7 @@ public:
                                e->energy};
         check(vlj_set_heat_exchange(sim_, &h));
     }
+    void set_grid_every_step(bool on) { check(vlj_set_grid_every_step(sim_, on ? 1 : 0)); }
     std::optional<double> heat_flux() const {
         int has = 0;
         double f = 0.0;

@@ -261,3 +261,39 @@ def test_kernel_counter_counts_skipped_rebuilds_out(gpu):
     # a step kernel per step, a decide per 16-step graph (the step kernels take
     # the later steps' decisions), six per rebuild
     assert k1 - k0 == 64 + 64 // 16 + 6 * (r1 - r0)
+
+
+def test_grid_every_step_keeps_the_trajectory(gpu):
+    # the 256k workload's wording rebuilds the cell grid on every step; the
+    # reference bins only with the lists. Both give the same lists and the
+    # same trajectory to the bit; the grid kernels run on every step.
+    p, L = gpu.lattice_fcc(10, 0.8442, 1.0, 7)
+    settings = gpu.Settings([L] * 3, dt=0.005, shifted_force=True,
+                            thermostat=gpu.Langevin(1.0, 1.0, 7))
+    plain, every = gpu.LennardJones(p, settings), gpu.LennardJones(p, settings)
+    every.set_grid_every_step(True)
+    direct = gpu.LennardJones(p, settings)
+    direct.set_grid_every_step(True)
+    direct.set_graphs(False)
+    r0 = plain.measure_now().list_rebuilds
+    every.measure_now()
+    k_plain, k_every = plain.kernels_executed(), every.kernels_executed()
+    for sim in (plain, every, direct):
+        sim.run(200)
+    k_plain, k_every = plain.kernels_executed() - k_plain, every.kernels_executed() - k_every
+    # a step kernel per step, a decide per graph launch (12 of 16 steps, 8 of
+    # one), six more per rebuild
+    rebuilds, rest = divmod(k_plain - 200 - 20, 6)
+    assert rest == 0 and rebuilds > 0
+    ms = [sim.measure_now() for sim in (plain, every, direct)]
+    assert ms[0].list_rebuilds - r0 >= rebuilds
+    assert ms[0].list_rebuilds == ms[1].list_rebuilds == ms[2].list_rebuilds
+    assert (ms[0].potential, ms[0].virial, ms[0].kinetic) == (ms[1].potential, ms[1].virial, ms[1].kinetic)
+    assert (ms[0].potential, ms[0].virial) == (ms[2].potential, ms[2].virial)
+    q = [sim.read_particles() for sim in (plain, every, direct)]
+    for other in q[1:]:
+        assert np.array_equal(q[0]["pos"], other["pos"]) and np.array_equal(q[0]["vel"], other["vel"])
+    g0, g1 = plain.read_grid(), every.read_grid()
+    assert np.array_equal(g0["counts"], g1["counts"]) and np.array_equal(g0["lists"], g1["lists"])
+    # bin, scan, scatter and sort also on every step without a rebuild
+    assert k_every - k_plain == 4 * (200 - rebuilds)

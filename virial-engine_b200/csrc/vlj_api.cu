@@ -574,6 +574,27 @@ vlj_status vlj_set_heat_exchange(vlj_sim* s, const vlj_heat_exchange* exchange) 
 }
 
 // lennard_jones.rs:948-952: the energy moved per step (its f32 value) over 2 A dt.
+// Not in the reference, which bins only when the lists rebuild: rebuild the
+// cell grid (bin, scan, scatter, per-cell sort) on every step as well, the
+// lists still on the skin / 2 trigger. The trajectory is the same to the bit;
+// only the work per step changes. A single box only.
+vlj_status vlj_set_grid_every_step(vlj_sim* s, int on) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (!s->replicas.empty()) return fail(VLJ_NOT_ENABLED, "grid every step is for a single box");
+    const bool want = on != 0;
+    if (want == s->grid_every_step) return VLJ_OK;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
+    if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
+    s->graph_chunk = s->graph_one = nullptr;
+    const uint32_t flag = want ? 1u : 0u;
+    CUDA_TRY(cudaMemcpyAsync(&s->arena.glob->grid_every_step, &flag, sizeof flag,
+                             cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->grid_every_step = want;
+    return VLJ_OK;
+}
+
 vlj_status vlj_heat_flux(const vlj_sim* s, int* has, double* flux) {
     if (!s || !has || !flux) return fail(VLJ_INVALID_ARG, "null argument");
     *has = s->exchange ? 1 : 0;
@@ -967,6 +988,11 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         } else {
             n_decide = prev;  // the previous step kernel decided
         }
+        if (s->grid_every_step) {
+            // the cell grid on every step, ahead of the conditional lists
+            CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_decide, nullptr, 1, mode));
+            TRY(end_capture(cs, launch_grid(s->arena, cs), &n_decide));
+        }
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.conditional.handle = h[k];
         cp.conditional.type = cudaGraphCondTypeIf;
@@ -974,7 +1000,9 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         CUDA_TRY(cudaGraphAddNode(&n_cond, g, &n_decide, 1, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
-        TRY(end_capture(cs, launch_rebuild(s->arena, cs), nullptr));
+        TRY(end_capture(cs, s->grid_every_step ? launch_lists(s->arena, cs)
+                                               : launch_rebuild(s->arena, cs),
+                        nullptr));
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
         cudaError_t e;
         if (fold)

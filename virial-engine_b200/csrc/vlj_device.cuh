@@ -36,6 +36,12 @@ __device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
     return a.ctrl[b].rebuild != 0u;
 }
 
+// Whether the cell grid is rebuilt this step: with the lists, or on every
+// step when grid_every_step is set (a single box).
+__device__ __forceinline__ bool grid_pass(const Arena& a) {
+    return a.glob->any != 0u || a.glob->grid_every_step != 0u;
+}
+
 // ---- decide (lennard_jones.wgsl:281-307), by one whole block ----
 // Finishes the previous step's bookkeeping (flip the position copy, advance
 // the step counter), then per box: rebuild when something moved more than
@@ -78,7 +84,9 @@ __device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditiona
     __syncthreads();
     if (a.nboxes == 1u) {
         if (threadIdx.x == 0) {
-            const bool r = a.ctrl[0].rebuild != 0u;
+            // the particles the grid kernels cover: the box's, when its lists
+            // rebuild or its grid is rebuilt every step
+            const bool r = a.ctrl[0].rebuild != 0u || g->grid_every_step != 0u;
             a.rb_box[0] = 0u;
             a.rb_first[0] = 0u;
             a.rb_first[r ? 1 : 0] = r ? a.boxes[0].n : 0u;

@@ -98,7 +98,7 @@ __global__ void decide_kernel(Arena a, cudaGraphConditionalHandle handle) {
 // ---- bin (grid.wgsl:11-38): cell of each slot from its f32 position ----
 __global__ void bin_kernel(Arena a) {
     count_kernel(a);
-    if (!a.glob->any) return;
+    if (!grid_pass(a)) return;
     for_rebuild_slots(a, [&](uint32_t i, uint32_t b) {
         const Box& bx = a.boxes[b];
         int32_t c[3];
@@ -115,7 +115,7 @@ __global__ void bin_kernel(Arena a) {
         atomicAdd(&a.count[cell], 1u);
 #if !VLJ_LIST_STREAM
         // a force block wholly inside this box restarts its staged-row count
-        if (i % kForceThreads == 0u) {
+        if (i % kForceThreads == 0u && rebuilding(a, b)) {
             const uint32_t end = min(i + (uint32_t)kForceThreads, a.nslots);
             if (i >= bx.first && end <= bx.first + bx.n) a.block_rows[i / kForceThreads] = 0u;
         }
@@ -132,9 +132,9 @@ constexpr int kScanPer = 16;  // counts per thread: a box of up to 16,384 cells 
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     count_kernel(a);
-    if (!a.glob->any) return;
+    if (!grid_pass(a)) return;
     uint32_t b = blockIdx.x;
-    if (b >= a.nboxes || !rebuilding(a, b)) return;
+    if (b >= a.nboxes || !(rebuilding(a, b) || a.glob->grid_every_step)) return;
     const Box& bx = a.boxes[b];
     __shared__ uint32_t s_warp[kScanThreads / 32];
     __shared__ uint32_t s_carry;
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
 // ---- scatter (grid.wgsl:119-127): slot into its cell's next free place ----
 __global__ void scatter_kernel(Arena a) {
     count_kernel(a);
-    if (!a.glob->any) return;
+    if (!grid_pass(a)) return;
     for_rebuild_slots(a, [&](uint32_t i, uint32_t) {
         const uint32_t c = a.cell_of_slot[i];
         a.sorted[a.cell_start[c] + atomicAdd(&a.count[c], 1u)] = i;
@@ -266,7 +266,7 @@ __device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, u
 
 __global__ void sort_kernel(Arena a) {
     count_kernel(a);
-    if (!a.glob->any) return;
+    if (!grid_pass(a)) return;
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t cells = a.glob->work_cells;
@@ -381,7 +381,7 @@ cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long con
     return after_launch();
 }
 
-cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
+cudaError_t launch_grid(const Arena& a, cudaStream_t s) {
     // the per-particle kernels cover the rebuilding boxes' particles from a
     // resident grid
     const unsigned slots = (unsigned)sm_count() * 8u;
@@ -389,9 +389,18 @@ cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
     scan_kernel<<<a.nboxes, kScanThreads, 0, s>>>(a);
     scatter_kernel<<<slots, kBlock, 0, s>>>(a);
     sort_kernel<<<(unsigned)sm_count() * 8u, kBlock, 0, s>>>(a);
-    reorder_kernel<<<slots, kBlock, 0, s>>>(a);
+    return after_launch(4);
+}
+
+cudaError_t launch_lists(const Arena& a, cudaStream_t s) {
+    reorder_kernel<<<(unsigned)sm_count() * 8u, kBlock, 0, s>>>(a);
     launch_build_list(a, s);  // vlj_build.cu
-    return after_launch(6);
+    return after_launch(2);
+}
+
+cudaError_t launch_rebuild(const Arena& a, cudaStream_t s) {
+    const cudaError_t e = launch_grid(a, s);
+    return e != cudaSuccess ? e : launch_lists(a, s);
 }
 
 }  // namespace vlj

@@ -130,7 +130,7 @@ struct Global {
     uint32_t fault;      // first error a kernel recorded (0 none)
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
-    uint32_t unused;
+    uint32_t grid_every_step;    // 1: bin, scan, scatter and sort every step (one box)
     uint32_t work_cells;         // entries of Arena::work this step
     uint32_t next_build;         // next work entry the list build takes
     uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
@@ -395,6 +395,10 @@ cudaError_t launch_load_particles(const Arena& a, cudaStream_t s);
 cudaError_t launch_store_particles(const Arena& a, cudaStream_t s);
 cudaError_t launch_decide(const Arena& a, cudaStream_t s, unsigned long long cond_handle);
 cudaError_t launch_rebuild(const Arena& a, cudaStream_t s);
+// The two halves of launch_rebuild: the cell grid (bin, scan, scatter, sort)
+// and the lists (reorder copy-back, list build).
+cudaError_t launch_grid(const Arena& a, cudaStream_t s);
+cudaError_t launch_lists(const Arena& a, cudaStream_t s);
 // The force kernels read list rows through `list_map`: a 2D TMA tensor map
 // over the list viewed as u64 pairs of entries (inner dimension 2 * seg,
 // outer one row per four entries) whose box is kTileRows rows of

@@ -41,6 +41,7 @@ struct vlj_sim {
     bool exchange = false;     // heat exchange on (constant energy, canonical velocities)
     vlj_heat_exchange exchange_settings{};
     bool canonical() const { return nose_hoover || exchange; }
+    bool grid_every_step = false;  // bin, scan, scatter, sort every step; lists on the trigger
     vlj::Box box{};
     // batched: one Box per replica, in slot order (empty for a single box)
     std::vector<vlj::Box> replicas;

@@ -386,6 +386,12 @@ class LennardJones:
         _check(_lib.vlj_heat_flux(self._h, C.byref(has), C.byref(f)))
         return f.value if has.value else None
 
+    def set_grid_every_step(self, on):
+        """Rebuild the cell grid on every step as well (the lists still on the
+        skin / 2 trigger): the same trajectory, more work per step. Not in the
+        reference, which bins only when the lists rebuild."""
+        _check(_lib.vlj_set_grid_every_step(self._h, int(bool(on))))
+
     # profiles
     def sample_profile(self):
         _check(_lib.vlj_sample_profile(self._h))

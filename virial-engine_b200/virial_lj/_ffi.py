@@ -83,6 +83,7 @@ SIGNATURES = {
     "vlj_set_temperature": [_vp, C.c_double],
     "vlj_set_heat_exchange": [_vp, _P(HeatExchange)],
     "vlj_heat_flux": [_vp, _P(C.c_int), _P(C.c_double)],
+    "vlj_set_grid_every_step": [_vp, C.c_int],
     "vlj_sample_profile": [_vp],
     "vlj_clear_profile": [_vp],
     "vlj_read_profile": [_vp, _P(Slab), _P(C.c_double), _P(C.c_uint64)],
