@@ -126,111 +126,89 @@ __global__ void bin_kernel(Arena a) {
 // ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
 // the counts offset by the box's first slot; counts become zeroed cursors.
 // The box's non-empty cells join the step's work list for the sort and the
-// list build.
+// list build. Each warp takes kScanPer runs of 32 consecutive cells, a lane
+// per cell, so every load and store of a run is one coalesced line; shuffles
+// scan within the warp, warp 0 scans the warps' totals, and one atomic per
+// block reserves its work-list entries.
 constexpr int kScanThreads = 1024;
-constexpr int kScanPer = 16;  // counts per thread: a box of up to 16,384 cells in one pass
+constexpr int kScanPer = 16;  // runs of 32 cells per warp: 16,384 cells per pass
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     count_kernel(a);
     if (!grid_pass(a)) return;
-    uint32_t b = blockIdx.x;
+    const uint32_t b = blockIdx.x;
     if (b >= a.nboxes || !(rebuilding(a, b) || a.glob->grid_every_step)) return;
     const Box& bx = a.boxes[b];
-    __shared__ uint32_t s_warp[kScanThreads / 32];
-    __shared__ uint32_t s_carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ uint32_t s_sum[kScanThreads / 32], s_nz[kScanThreads / 32];
+    __shared__ uint32_t s_carry, s_tile;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
     if (threadIdx.x == 0) s_carry = bx.first;
     __syncthreads();
     const uint32_t total = bx.total_cells, base = bx.cell_base;
-    for (uint32_t tile = 0; tile < total; tile += kScanThreads * kScanPer) {
-        uint32_t v[kScanPer];
-        uint32_t sum = 0;
-        const uint32_t c_first = tile + threadIdx.x * kScanPer;
-        // a thread's counts as 16-byte loads where they are aligned and whole
-        // (a single box starts at cell 0)
-        const bool vec = (base & 3u) == 0u && c_first + kScanPer <= total;
-        if (vec) {
-            const uint4* p = reinterpret_cast<const uint4*>(a.count + base + c_first);
+    for (uint32_t tile = 0; tile < total; tile += (uint32_t)kScanThreads * kScanPer) {
+        const uint32_t first = tile + warp * 32u * (uint32_t)kScanPer;
+        uint32_t excl[kScanPer];  // within the warp's cells, before this lane's
+        uint32_t nonempty = 0;    // bit r: this lane's cell of run r holds particles
+        uint32_t sum = 0, nz = 0;
 #pragma unroll
-            for (int r = 0; r < kScanPer / 4; r++) {
-                const uint4 w = p[r];
-                v[4 * r] = w.x;
-                v[4 * r + 1] = w.y;
-                v[4 * r + 2] = w.z;
-                v[4 * r + 3] = w.w;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kScanPer; q++) {
-                const uint32_t c = c_first + q;
-                v[q] = c < total ? a.count[base + c] : 0u;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kScanPer; q++) sum += v[q];
-        // inclusive scan of the per-thread sums
-        uint32_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) s_warp[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = s_warp[lane];
+        for (int r = 0; r < kScanPer; r++) {
+            const uint32_t c = first + 32u * (uint32_t)r + lane;
+            const uint32_t v = c < total ? a.count[base + c] : 0u;
+            uint32_t x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += t;
+                const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= (uint32_t)o) x += t;
             }
-            s_warp[lane] = w;
+            excl[r] = sum + x - v;
+            sum += __shfl_sync(0xffffffffu, x, 31);
+            const unsigned m = __ballot_sync(0xffffffffu, v != 0u);
+            nonempty |= (v != 0u ? 1u : 0u) << r;
+            nz += (uint32_t)__popc(m);
+        }
+        if (lane == 0) {
+            s_sum[warp] = sum;
+            s_nz[warp] = nz;
         }
         __syncthreads();
-        uint32_t before = s_carry + (warp ? s_warp[warp - 1] : 0u) + incl - sum;
-        if (vec) {
-            uint4* st = reinterpret_cast<uint4*>(a.cell_start + base + c_first);
-            uint4* zero = reinterpret_cast<uint4*>(a.count + base + c_first);
+        if (warp == 0) {
+            const uint32_t ws = s_sum[lane], wn = s_nz[lane];
+            uint32_t is = ws, in = wn;
 #pragma unroll
-            for (int r = 0; r < kScanPer / 4; r++) {
-                uint4 w;
-                w.x = before;
-                w.y = w.x + v[4 * r];
-                w.z = w.y + v[4 * r + 1];
-                w.w = w.z + v[4 * r + 2];
-                before = w.w + v[4 * r + 3];
-                st[r] = w;
-                zero[r] = make_uint4(0u, 0u, 0u, 0u);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kScanPer; q++) {
-                const uint32_t c = c_first + q;
-                if (c < total) {
-                    a.cell_start[base + c] = before;
-                    a.count[base + c] = 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t ts = __shfl_up_sync(0xffffffffu, is, o);
+                const uint32_t tn = __shfl_up_sync(0xffffffffu, in, o);
+                if (lane >= (uint32_t)o) {
+                    is += ts;
+                    in += tn;
                 }
-                before += v[q];
             }
+            const uint32_t block_nz = __shfl_sync(0xffffffffu, in, 31);
+            uint32_t at = 0;
+            if (lane == 0 && block_nz) at = atomicAdd(&a.glob->work_cells, block_nz);
+            at = __shfl_sync(0xffffffffu, at, 0);
+            s_sum[lane] = is - ws;
+            s_nz[lane] = at + in - wn;
+            if (lane == 31u) s_tile = is;
         }
-        // append the non-empty cells to the work list: one atomic per warp
-        uint32_t nz = 0;
-#pragma unroll
-        for (int q = 0; q < kScanPer; q++) nz += v[q] ? 1u : 0u;
-        uint32_t nz_incl = nz;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, nz_incl, o);
-            if (lane >= o) nz_incl += t;
-        }
-        uint32_t at = 0;
-        if (lane == 31 && nz_incl) at = atomicAdd(&a.glob->work_cells, nz_incl);
-        at = __shfl_sync(0xffffffffu, at, 31) + nz_incl - nz;
-#pragma unroll
-        for (int q = 0; q < kScanPer; q++)
-            if (v[q]) a.work[at++] = base + tile + threadIdx.x * kScanPer + q;
         __syncthreads();
-        if (threadIdx.x == 0) s_carry += s_warp[kScanThreads / 32 - 1];
+        const uint32_t before = s_carry + s_sum[warp];
+        uint32_t at = s_nz[warp];
+#pragma unroll
+        for (int r = 0; r < kScanPer; r++) {
+            const uint32_t c = first + 32u * (uint32_t)r + lane;
+            if (c < total) {
+                a.cell_start[base + c] = before + excl[r];
+                a.count[base + c] = 0u;
+            }
+            const bool keep = (nonempty >> r) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (keep) a.work[at + (uint32_t)__popc(m & below)] = base + c;
+            at += (uint32_t)__popc(m);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += s_tile;
         __syncthreads();
     }
 }
