@@ -170,6 +170,51 @@ def test_heat_current_matches_f64(gpu, O):
     assert sim.read_heat_current().shape == (0, 3)
 
 
+@pytest.mark.parametrize("shifted_force", [False, True])
+def test_heat_current_taken_by_the_next_step(gpu, O, shifted_force):
+    # A sample requested between steps is taken by the next step's force pass
+    # (the state it starts from); before anything else reads the series or
+    # changes the state, by the sampling kernel. Both give the f64 current.
+    size = [9.0, 9.0, 12.0]
+    count = int(round(0.8442 * 9 * 9 * 12))
+    pos, vel = O.lattice_box(count, size, 1.0, 11)
+    fused = make(gpu, pos, vel, size, shifted_force=shifted_force, dt=0.002)
+    alone = make(gpu, pos, vel, size, shifted_force=shifted_force, dt=0.002)
+    direct = make(gpu, pos, vel, size, shifted_force=shifted_force, dt=0.002)
+    direct.set_graphs(False)
+    scale = np.sqrt(count) * 10.0
+    refs = []
+    for sim in (fused, alone, direct):
+        sim.run(300)
+        sim.record_heat_current(24)
+    for k in range(24):
+        if k % 8 == 0:
+            wp, v, box = canonical(fused)
+            refs.append((k, O.heat_current(wp, v, box, 2.5, shifted_force)))
+        for sim in (fused, alone, direct):
+            sim.sample_heat_current()
+        alone.read_heat_current()  # takes its sample now, with the sampling kernel
+        for sim in (fused, alone, direct):
+            sim.step(1)
+    jf, ja, jd = fused.read_heat_current(), alone.read_heat_current(), direct.read_heat_current()
+    assert jf.shape == ja.shape == (24, 3)
+    assert np.array_equal(jf, jd)  # captured and direct steps: the same kernel
+    assert np.abs(jf - ja).max() < 1e-5 * scale, np.abs(jf - ja).max()
+    for k, ref in refs:
+        assert np.abs(jf[k] - ref).max() < 1e-5 * scale, (k, jf[k], ref)
+    # taking the sample changes nothing in the trajectory
+    qf, qa = fused.read_particles(), alone.read_particles()
+    assert np.array_equal(qf["pos"], qa["pos"]) and np.array_equal(qf["vel"], qa["vel"])
+    # a sample pending when the state is overwritten is taken first
+    fused.record_heat_current(2)
+    fused.sample_heat_current()
+    wp, v, box = canonical(fused)
+    ref = O.heat_current(wp, v, box, 2.5, shifted_force)
+    fused.write_particles(fused.read_particles())
+    j = fused.read_heat_current()
+    assert j.shape == (1, 3) and np.abs(j[0] - ref).max() < 1e-5 * scale
+
+
 def test_sampling_errors(gpu, O):
     pos, vel = O.lattice(1000, 11.0, 1.0, 3)
     sim = make(gpu, pos, vel, [11.0] * 3)

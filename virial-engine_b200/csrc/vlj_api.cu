@@ -281,6 +281,7 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
 vlj_sim::~vlj_sim() {
     if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
     if (graph_one) cudaGraphExecDestroy(graph_one);
+    if (graph_one_heat) cudaGraphExecDestroy(graph_one_heat);
     if (graph_lists) cudaGraphExecDestroy(graph_lists);
     if (capture_stream) cudaStreamDestroy(capture_stream);
     for (cudaEvent_t e : ev_start) cudaEventDestroy(e);
@@ -438,6 +439,7 @@ vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
 vlj_status vlj_write_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
     if (!s || !p) return fail(VLJ_INVALID_ARG, "null argument");
     if (count != s->n) return fail(VLJ_INVALID_ARG, "expected %u particles, got %zu", s->n, count);
+    TRY(sim_flush_heat(s));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return restart(s, p, count);
 }
@@ -543,11 +545,10 @@ vlj_status vlj_set_heat_exchange(vlj_sim* s, const vlj_heat_exchange* exchange) 
             return fail(VLJ_INVALID_ARG, "energy must be finite");
     }
     const bool on = exchange != nullptr;
+    TRY(sim_flush_heat(s));
     if (on != s->exchange) {
         CUDA_TRY(cudaStreamSynchronize(s->stream));
-        if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
-        if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
-        s->graph_chunk = s->graph_one = nullptr;
+        sim_drop_step_graphs(s);
     }
     if (on) {
         s->box.hex_slabs[0] = (float)exchange->hot[0];
@@ -584,9 +585,7 @@ vlj_status vlj_set_grid_every_step(vlj_sim* s, int on) {
     const bool want = on != 0;
     if (want == s->grid_every_step) return VLJ_OK;
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
-    if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
-    s->graph_chunk = s->graph_one = nullptr;
+    sim_drop_step_graphs(s);
     const uint32_t flag = want ? 1u : 0u;
     CUDA_TRY(cudaMemcpyAsync(&s->arena.glob->grid_every_step, &flag, sizeof flag,
                              cudaMemcpyHostToDevice, s->stream));
@@ -960,7 +959,8 @@ static cudaError_t launch_step_tail(vlj_sim* s, cudaStream_t cs) {
 // step kernel, chained (canonical velocities: begin -> decide -> IF{...} ->
 // canon_force [-> hex_apply]). The decide kernel sets the condition on the device, so a step
 // with no rebuild launches no rebuild kernel at all.
-static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) {
+static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out,
+                              bool heat = false) {
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaGraphCreate(&g, 0));
     struct Guard {
@@ -1007,7 +1007,7 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out) 
         cudaError_t e;
         if (fold)
             e = launch_step(s->arena, s->list_map, s->shifted_force, cs,
-                            k + 1 < count ? (unsigned long long)h[k + 1] : 0ull);
+                            k + 1 < count ? (unsigned long long)h[k + 1] : 0ull, heat && k == 0);
         else
             e = launch_step_tail(s, cs);
         TRY(end_capture(cs, e, &prev));
@@ -1045,7 +1045,7 @@ vlj_status sim_launch_lists_graph(vlj_sim* s) {
     return VLJ_OK;
 }
 
-static vlj_status step_direct(vlj_sim* s) {
+static vlj_status step_direct(vlj_sim* s, bool heat = false) {
     if (s->canonical()) {
         CUDA_TRY(launch_begin(s->arena, s->stream));
         CUDA_TRY(launch_decide(s->arena, s->stream, 0));
@@ -1064,16 +1064,27 @@ static vlj_status step_direct(vlj_sim* s) {
             s->ev_end.push_back(b);
         }
         CUDA_TRY(cudaEventRecord(s->ev_start[s->ev_used], s->stream));
-        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream));
+        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream, 0, heat));
         CUDA_TRY(cudaEventRecord(s->ev_end[s->ev_used], s->stream));
         s->ev_used++;
     } else {
-        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream));
+        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream, 0, heat));
     }
     return VLJ_OK;
 }
 
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
+    if (steps > 0 && s->heat_pending) {
+        // the first step's force pass takes the requested heat-current sample
+        s->heat_pending = false;
+        if (s->timing || !s->use_graphs) {
+            TRY(step_direct(s, true));
+        } else {
+            if (!s->graph_one_heat) TRY(build_graph(s, 1, &s->graph_one_heat, true));
+            CUDA_TRY(cudaGraphLaunch(s->graph_one_heat, s->stream));
+        }
+        steps -= 1;
+    }
     if (s->timing || !s->use_graphs) {
         for (uint32_t k = 0; k < steps; k++) TRY(step_direct(s));
         return VLJ_OK;
@@ -1084,6 +1095,21 @@ vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
         CUDA_TRY(cudaGraphLaunch(s->graph_chunk, s->stream));
     for (; steps > 0; steps--) CUDA_TRY(cudaGraphLaunch(s->graph_one, s->stream));
     return VLJ_OK;
+}
+
+vlj_status sim_flush_heat(vlj_sim* s) {
+    if (!s->heat_pending) return VLJ_OK;
+    s->heat_pending = false;
+    TRY(lists_now(s));
+    CUDA_TRY(launch_heat_current(s->arena, s->shifted_force, s->series_samples - 1u, s->stream));
+    return VLJ_OK;
+}
+
+void sim_drop_step_graphs(vlj_sim* s) {
+    if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
+    if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
+    if (s->graph_one_heat) cudaGraphExecDestroy(s->graph_one_heat);
+    s->graph_chunk = s->graph_one = s->graph_one_heat = nullptr;
 }
 
 }  // namespace vlj

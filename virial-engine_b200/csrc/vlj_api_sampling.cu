@@ -90,6 +90,7 @@ vlj_status vlj_read_profile(vlj_sim* s, vlj_slab* slabs, double virial[3], uint6
 // lennard_jones.rs:954-974: room for `capacity` samples, earlier ones dropped
 vlj_status vlj_record_heat_current(vlj_sim* s, uint32_t capacity) {
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    s->heat_pending = false;  // a sample of the series being dropped
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (s->series) {
         cudaFree(s->series);
@@ -104,6 +105,9 @@ vlj_status vlj_record_heat_current(vlj_sim* s, uint32_t capacity) {
     s->arena.series_capacity = capacity;
     s->series_capacity = capacity;
     s->series_samples = 0;
+    CUDA_TRY(cudaMemsetAsync(&s->arena.glob->heat_next, 0, sizeof(uint32_t), s->stream));
+    // the captured steps hold the old series' address
+    sim_drop_step_graphs(s);
     return VLJ_OK;
 }
 
@@ -113,8 +117,14 @@ vlj_status vlj_sample_heat_current(vlj_sim* s) {
     if (!s->series) return fail(VLJ_NOT_ENABLED, "record_heat_current first");
     if (s->series_samples >= s->series_capacity)
         return fail(VLJ_FULL, "heat current series full");
-    TRY(sim_lists_now(s));
-    CUDA_TRY(launch_heat_current(s->arena, s->shifted_force, s->series_samples, s->stream));
+    TRY(sim_flush_heat(s));
+    if (s->canonical()) {
+        TRY(sim_lists_now(s));
+        CUDA_TRY(launch_heat_current(s->arena, s->shifted_force, s->series_samples, s->stream));
+    } else {
+        // taken by the next step's force pass, which sees this same state
+        s->heat_pending = true;
+    }
     s->series_samples += 1;
     return VLJ_OK;
 }
@@ -123,6 +133,7 @@ vlj_status vlj_sample_heat_current(vlj_sim* s) {
 vlj_status vlj_read_heat_current(vlj_sim* s, double* out, size_t capacity, size_t* samples) {
     if (!s || !samples) return fail(VLJ_INVALID_ARG, "null argument");
     if (!s->series) return fail(VLJ_NOT_ENABLED, "record_heat_current first");
+    TRY(sim_flush_heat(s));
     const size_t n = s->series_samples;
     std::vector<long long> raw(1 + 3 * n);
     CUDA_TRY(cudaMemcpyAsync(raw.data(), s->series, raw.size() * sizeof(long long),

@@ -33,6 +33,9 @@ struct PairSums {
     float pe, pe_lo;  // this particle's half of its pair energies, hi + lo
     float w, w_lo;    // and of its pair virials r . F
     uint32_t near;    // neighbours within 1.5 sigma
+    // heat current: half of the pair energies, and T = sum_j d d^T |F| / r
+    // (xx yy zz xy xz yz)
+    float e_half, t[6];
 };
 
 // Shared memory of a force-kernel block: the tile ring and its barriers
@@ -117,11 +120,12 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
 // also summed, as unevaluated f32 pairs (as the reference sums them in
 // double-float, lennard_jones.wgsl:518-519). Every thread of the block must
 // call this: it synchronises the block between tiles.
-template <bool SHIFTED_FORCE, bool ENERGIES>
+template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT = false>
 __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap* map,
                                                     const Arena& a, const Box& bx, uint32_t i,
                                                     bool valid, const uint4* __restrict__ cur) {
-    PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u};
+    PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u,
+                  0.0f, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}};
 #if !VLJ_LIST_STREAM
     const uint32_t first = blockIdx.x * kForceThreads;
     const uint32_t rows = a.block_rows[blockIdx.x];
@@ -156,14 +160,24 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         const float dx = decode_diff(pj.x, own.x, dec0);
         const float dy = decode_diff(pj.y, own.y, dec1);
         const float dz = decode_diff(pj.z, own.z, dec2);
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = sep_r2(dx, dy, dz);
         const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
         // branch-free: most list entries are inside the cutoff; the select
         // drops whatever the pair math gives for entries that are not
         const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
-        s.ax -= dx * f;
-        s.ay -= dy * f;
-        s.az -= dz * f;
+        s.ax = __fmaf_rn(-dx, f, s.ax);
+        s.ay = __fmaf_rn(-dy, f, s.ay);
+        s.az = __fmaf_rn(-dz, f, s.az);
+        if (HEAT) {
+            s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
+            const float fx = dx * f, fy = dy * f, fz = dz * f;
+            s.t[0] += dx * fx;
+            s.t[1] += dy * fy;
+            s.t[2] += dz * fz;
+            s.t[3] += dx * fy;
+            s.t[4] += dx * fz;
+            s.t[5] += dy * fz;
+        }
         if (ENERGIES && in) {
             // The sums take r^2 rounded once from the exact separation (the
             // integer differences times the box step are exact in f64): on a
@@ -277,6 +291,27 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
 #endif
 }
 
+// Sum of one heat-current sample's three components over the block into
+// series slot 1 + 3 * sample: one atomic each (integer sums, any order).
+__device__ __forceinline__ void block_sum_series(const Arena& a, const long long (&raw)[3],
+                                                 uint32_t sample) {
+    __shared__ long long s_sum[kForceThreads / 32][3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        long long x = raw[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) s_sum[warp][c] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        long long x = 0;
+        for (int w = 0; w < kForceThreads / 32; w++) x += s_sum[w][threadIdx.x];
+        if (x) atomicAdd(&a.series[1 + 3 * (size_t)sample + threadIdx.x], (unsigned long long)x);
+    }
+}
+
 // Langevin noise of a particle at a step: Philox-4x32-10 (Salmon et al.,
 // SC'11) with counter (id, step lo, step hi, 0) and key (seed, "LJV1");
 // uniforms in (0, 1] from 24 bits as the reference's uniform01
@@ -328,7 +363,7 @@ __global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
 // The new position goes to the other cache copy (neighbours still read this
 // step's), and the largest squared displacement since the last list build
 // feeds the next step's rebuild decision.
-template <bool SHIFTED_FORCE>
+template <bool SHIFTED_FORCE, bool HEAT>
 __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Arena a,
                                                              const __grid_constant__ CUtensorMap map,
                                                              cudaGraphConditionalHandle next) {
@@ -339,7 +374,29 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     const uint32_t phase = a.glob->phase;
     const uint32_t b = valid ? box_of_slot(a, i) : 0u;
     const Box& bx = a.boxes[b];
-    const PairSums s = block_pair_sums<SHIFTED_FORCE, false>(st, &map, a, bx, i, valid, a.cache[phase]);
+    const PairSums s =
+        block_pair_sums<SHIFTED_FORCE, false, HEAT>(st, &map, a, bx, i, valid, a.cache[phase]);
+    if (HEAT) {
+        // the heat current of the state this step starts from, as the
+        // sampling kernel would take it: J_i = e_i v_i + T_i v_i / 2 with the
+        // canonical velocity v_i = v + a dt / 2 (one box, velocities half a
+        // kick behind)
+        const uint32_t sample = a.glob->heat_next;
+        long long raw[3] = {0, 0, 0};
+        if (valid) {
+            const float acc3[3] = {s.ax, s.ay, s.az};
+            double v[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[c] = canonical_velocity(a, bx, 0, i, c, acc3[c]);
+            const double e = 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + (double)s.e_half;
+            const double tv[3] = {s.t[0] * v[0] + s.t[3] * v[1] + s.t[4] * v[2],
+                                  s.t[3] * v[0] + s.t[1] * v[1] + s.t[5] * v[2],
+                                  s.t[4] * v[0] + s.t[5] * v[1] + s.t[2] * v[2]};
+#pragma unroll
+            for (int c = 0; c < 3; c++) raw[c] = fixed_raw_f64(e * v[c] + 0.5 * tv[c]);
+        }
+        block_sum_series(a, raw, sample);
+    }
     float disp2 = 0.0f;
     if (valid) {
         const float acc[3] = {s.ax, s.ay, s.az};
@@ -372,8 +429,9 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     }
     block_max_per_box(a, valid, b, blockIdx.x * kForceThreads, disp2);
     if (i == 0) a.glob->pending = 1u;
-    if (!next) return;
-    // the last block to finish takes the next step's rebuild decision
+    if (!next && !HEAT) return;
+    // the last block to finish takes the next step's rebuild decision and
+    // moves the heat-current series on
     __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -383,8 +441,11 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    if (threadIdx.x == 0) a.glob->blocks_done = 0u;
-    decide_block(a, next, true);
+    if (threadIdx.x == 0) {
+        a.glob->blocks_done = 0u;
+        if (HEAT) a.glob->heat_next += 1u;
+    }
+    if (next) decide_block(a, next, true);
 }
 
 // ---- measure (lennard_jones.wgsl:576-626) ----
@@ -716,8 +777,10 @@ static void prefer_l1_once() {
     static bool done = false;
     if (done) return;
     done = true;
-    prefer_l1(step_kernel<true>);
-    prefer_l1(step_kernel<false>);
+    prefer_l1(step_kernel<true, false>);
+    prefer_l1(step_kernel<false, false>);
+    prefer_l1(step_kernel<true, true>);
+    prefer_l1(step_kernel<false, true>);
     prefer_l1(measure_kernel<true>);
     prefer_l1(measure_kernel<false>);
     prefer_l1(prime_kernel<true>);
@@ -743,13 +806,17 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_fo
 }
 
 cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
-                        cudaStream_t s, unsigned long long next_decision) {
+                        cudaStream_t s, unsigned long long next_decision, bool heat) {
     prefer_l1_once();
     const cudaGraphConditionalHandle next = (cudaGraphConditionalHandle)next_decision;
-    if (shifted_force)
-        step_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, next);
-    else
-        step_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map, next);
+    const unsigned blocks = particle_blocks(a);
+    if (shifted_force) {
+        if (heat) step_kernel<true, true><<<blocks, kForceThreads, 0, s>>>(a, map, next);
+        else step_kernel<true, false><<<blocks, kForceThreads, 0, s>>>(a, map, next);
+    } else {
+        if (heat) step_kernel<false, true><<<blocks, kForceThreads, 0, s>>>(a, map, next);
+        else step_kernel<false, false><<<blocks, kForceThreads, 0, s>>>(a, map, next);
+    }
     return after_launch();
 }
 

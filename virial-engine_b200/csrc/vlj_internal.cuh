@@ -136,6 +136,8 @@ struct Global {
     uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
     uint32_t rb_boxes;           // boxes that rebuild this step (Arena::rb_box)
     uint32_t rb_slots;           // their particles, in all
+    uint32_t heat_next;          // heat-current samples written to the series so far
+    uint32_t pad;
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).
@@ -345,20 +347,44 @@ __device__ __forceinline__ float rcp_pair(float x) {
 #endif
 }
 
+// The pair energy at r2 < rc2 with the force kernels' reciprocal (the same
+// approximations as lj_force_over_r2, so a pass computes both from one).
+template <bool SHIFTED_FORCE>
+__device__ __forceinline__ float lj_energy_fast(float r2, const Box& b) {
+    if (SHIFTED_FORCE) {
+        const float inv_r = rsqrt_pair(r2);
+        const float inv2 = inv_r * inv_r;
+        const float s6 = inv2 * inv2 * inv2;
+        return 4.0f * s6 * (s6 - 1.0f) - b.shift + (r2 * inv_r - b.rc) * b.force_shift;
+    }
+    const float inv2 = rcp_pair(r2);
+    const float s6 = inv2 * inv2 * inv2;
+    return 4.0f * s6 * (s6 - 1.0f) - b.shift;
+}
+
 // |F| / r of a pair at r2 < rc2: the factor that multiplies the separation.
+// Every operation is spelled out (no contraction left to the compiler), so
+// each kernel that computes it, whatever else it computes beside, gets the
+// same bits.
 template <bool SHIFTED_FORCE>
 __device__ __forceinline__ float lj_force_over_r2(float r2, float force_shift) {
     if (SHIFTED_FORCE) {
         // one reciprocal square root gives both 1/r^2 and r
         const float inv_r = rsqrt_pair(r2);
-        const float inv2 = inv_r * inv_r;
-        const float s6 = inv2 * inv2 * inv2;
-        const float rf = 24.0f * s6 * (2.0f * s6 - 1.0f) - r2 * inv_r * force_shift;
-        return rf * inv2;
+        const float inv2 = __fmul_rn(inv_r, inv_r);
+        const float s6 = __fmul_rn(__fmul_rn(inv2, inv2), inv2);
+        const float lj = __fmul_rn(__fmul_rn(24.0f, s6), __fmaf_rn(2.0f, s6, -1.0f));
+        const float rf = __fmaf_rn(-__fmul_rn(r2, inv_r), force_shift, lj);
+        return __fmul_rn(rf, inv2);
     }
     const float inv2 = rcp_pair(r2);
-    const float s6 = inv2 * inv2 * inv2;
-    return 24.0f * s6 * (2.0f * s6 - 1.0f) * inv2;
+    const float s6 = __fmul_rn(__fmul_rn(inv2, inv2), inv2);
+    return __fmul_rn(__fmul_rn(__fmul_rn(24.0f, s6), __fmaf_rn(2.0f, s6, -1.0f)), inv2);
+}
+
+// Squared length of a separation, the force kernels' way (spelled out).
+__device__ __forceinline__ float sep_r2(float dx, float dy, float dz) {
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
 }
 
 // The reference's nearest image d - side * round(d / side) with the IEEE
@@ -408,8 +434,12 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& list_map, bool shift
 // `next_decision`, when not 0, is the graph conditional of the next step's
 // rebuild: the step kernel's last block to finish then takes the next step's
 // decision itself (in place of a decide launch) and sets it.
+// With `heat`, the same kernel also takes the pending heat-current sample of
+// the state it starts from (series slot Global::heat_next, then advanced):
+// the force pass has every pair's separation and force, and the canonical
+// velocity v + a dt / 2 is known once the particle's forces are summed.
 cudaError_t launch_step(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
-                        cudaStream_t s, unsigned long long next_decision = 0);
+                        cudaStream_t s, unsigned long long next_decision = 0, bool heat = false);
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& list_map, bool shifted_force,
                            bool canonical, cudaStream_t s);
 // Steps on canonical velocities (one box): begin applies Nose-Hoover's

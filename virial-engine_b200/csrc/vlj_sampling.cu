@@ -30,12 +30,12 @@ __device__ __forceinline__ void walk_pairs(const Arena& a, const Box& bx, uint32
         const float dx = decode_diff(pj.x, own.x, bx.dec[0]);
         const float dy = decode_diff(pj.y, own.y, bx.dec[1]);
         const float dz = decode_diff(pj.z, own.z, bx.dec[2]);
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = sep_r2(dx, dy, dz);
         if (!(r2 < bx.rc2)) continue;
         const float f = lj_force_over_r2<SHIFTED_FORCE>(r2, bx.force_shift);
-        ax -= dx * f;
-        ay -= dy * f;
-        az -= dz * f;
+        ax = __fmaf_rn(-dx, f, ax);
+        ay = __fmaf_rn(-dy, f, ay);
+        az = __fmaf_rn(-dz, f, az);
         float rf, u;
         lj_pair<SHIFTED_FORCE>(r2, bx, rf, u);
         pair(dx, dy, dz, r2, rf, u);
@@ -132,6 +132,8 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kSampleThreads) heat_current_kernel(Arena a, uint32_t sample) {
     count_kernel(a);
+    // the series' count of written samples moves on (no other block reads it)
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.glob->heat_next = sample + 1u;
     const Box& bx = a.boxes[0];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < a.nslots;

@@ -58,6 +58,10 @@ struct vlj_sim {
     uint64_t profile_samples = 0;
     // heat current series
     uint32_t series_samples = 0;
+    // the last requested sample is not taken yet: the next step's force pass
+    // takes it (or, before anything that would change the state or read the
+    // series, the sampling kernel)
+    bool heat_pending = false;
     uint32_t series_capacity = 0;
     unsigned long long* series = nullptr;  // owned here (reallocated by record)
     // pinned staging for particle uploads and read-backs (x, v: 3 * seg; id: seg)
@@ -70,6 +74,7 @@ struct vlj_sim {
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph_chunk = nullptr;
     cudaGraphExec_t graph_one = nullptr;
+    cudaGraphExec_t graph_one_heat = nullptr;  // one step that also takes the pending sample
     cudaGraphExec_t graph_lists = nullptr;  // decide -> IF(rebuild){rebuild chain}
     // per-launch timing of the step kernel (direct launches while on)
     bool timing = false;
@@ -86,6 +91,10 @@ vlj_status make_list_map(const Arena& a, uint32_t rows, CUtensorMap* out);
 vlj_status sim_lists_now(vlj_sim* s);
 vlj_status check_fault(vlj_sim* s);
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
+// Takes a pending heat-current sample now, with the sampling kernel.
+vlj_status sim_flush_heat(vlj_sim* s);
+// Drops the captured step graphs (their shape changed).
+void sim_drop_step_graphs(vlj_sim* s);
 // The decision and, when due, the rebuild as one graph launch.
 vlj_status sim_launch_lists_graph(vlj_sim* s);
 }  // namespace vlj
