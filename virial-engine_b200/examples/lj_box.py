@@ -4,6 +4,7 @@ The reference's `examples/gas` drives LennardJones the same way (new, step,
 measure). Also the target of the committed ncu summaries in profiles/.
 
     python virial-engine_b200/examples/lj_box.py --cells 40 --steps 100
+    python virial-engine_b200/examples/lj_box.py --cells 10 --steps 1000 --record run1
 """
 
 import argparse
@@ -28,6 +29,10 @@ def main():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-graphs", action="store_true",
                     help="enqueue steps as direct launches (profilers see each kernel)")
+    ap.add_argument("--record", default=None, metavar="DIR",
+                    help="write measurements.csv (a row every --every steps), positions.npy "
+                         "and run.json into DIR, in the reference's formats")
+    ap.add_argument("--every", type=int, default=10)
     args = ap.parse_args()
     p, box = vl.lattice_fcc(args.cells, args.density, args.temperature, args.seed)
     thermostat = None if args.nve else vl.Langevin(args.temperature, 1.0, args.seed)
@@ -38,12 +43,50 @@ def main():
     m = sim.measure_now()
     print(f"{len(p)} particles, box {box:.4f}: E {m.energy():.6f} P {m.pressure():.6f}")
     t0 = time.perf_counter()
-    sim.run(args.steps)
+    if args.record:
+        record(sim, args, len(p), box)
+    else:
+        sim.run(args.steps)
     el = time.perf_counter() - t0
     m = sim.measure_now()
     print(f"after {args.steps} steps ({el * 1e6 / max(args.steps, 1):.1f} us/step wall): "
           f"E {m.energy():.6f} T {2 * m.kinetic / (3 * len(p)):.5f} P {m.pressure():.6f} "
           f"rebuilds {m.list_rebuilds} overflow {m.list_overflow}")
+
+
+def gpu_name():
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:  # no torch, or no device name to be had
+        return "unknown"
+
+
+def record(sim, args, n, box):
+    from virial_lj import data
+    log = data.DataLog(args.record)
+    dof = 3 * n if not args.nve else 3 * n - 3
+    done = 0
+    while True:
+        m = sim.measure_now()
+        log.row([("step", m.step), ("time", m.time), ("kinetic", m.kinetic),
+                 ("potential", m.potential), ("energy", m.energy()), ("virial", m.virial),
+                 ("temperature", m.temperature(dof)), ("pressure", m.pressure()),
+                 ("list_rebuilds", m.list_rebuilds)])
+        if done >= args.steps:
+            break
+        k = min(args.every, args.steps - done)
+        sim.run(k)
+        done += k
+    q = sim.read_particles()
+    log.snapshot("positions", q["pos"].shape, q["pos"])
+    log.meta("particles", n)
+    log.meta("box", data.exact(box))
+    settings = [("dt", args.dt), ("density", args.density), ("temperature", args.temperature),
+                ("thermostat", "none" if args.nve else "langevin"), ("seed", args.seed),
+                ("cutoff_style", "truncated-shifted" if args.truncated else "force-shifted")]
+    log.write(data.Manifest("lennard-jones box", gpu=gpu_name(), version="b200",
+                            frames=done, settings=settings))
 
 
 if __name__ == "__main__":
