@@ -105,13 +105,13 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     // Warps take home cells from the step's work list (the non-empty cells of
     // the boxes that rebuild) until it runs out.
-    const uint32_t cells = a.glob->work_cells;
+    const uint32_t cells = work_total(a), front = a.glob->work_front;
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(&a.glob->next_build, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= cells) break;
-        const uint32_t cell = a.work[t];
+        const uint32_t cell = work_item(a, front, t);
         const uint32_t b = box_of_cell(a, cell);
         const uint32_t hbeg = a.cell_start[cell], hend = a.cell_start[cell + 1];
         const Box& bx = a.boxes[b];

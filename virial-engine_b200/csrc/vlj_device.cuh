@@ -36,6 +36,15 @@ __device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
     return a.ctrl[b].rebuild != 0u;
 }
 
+// The step's work list: its length, and entry t (the dense cells first).
+__device__ __forceinline__ uint32_t work_total(const Arena& a) {
+    return a.glob->work_front + a.glob->work_back;
+}
+
+__device__ __forceinline__ uint32_t work_item(const Arena& a, uint32_t front, uint32_t t) {
+    return t < front ? a.work[t] : a.work[a.ncells - 1u - (t - front)];
+}
+
 // Whether the cell grid is rebuilt this step: with the lists, or on every
 // step when grid_every_step is set (a single box).
 __device__ __forceinline__ bool grid_pass(const Arena& a) {
@@ -55,7 +64,8 @@ __device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditiona
     Global* g = a.glob;
     if (threadIdx.x == 0) {
         s_any = 0;
-        g->work_cells = 0u;
+        g->work_front = 0u;
+        g->work_back = 0u;
         g->next_build = 0u;
         if (g->pending) {
             g->phase ^= 1u;

@@ -126,10 +126,11 @@ __global__ void bin_kernel(Arena a) {
 // ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
 // the counts offset by the box's first slot; counts become zeroed cursors.
 // The box's non-empty cells join the step's work list for the sort and the
-// list build. Each warp takes kScanPer runs of 32 consecutive cells, a lane
+// list build (cells of kDenseCell particles or more at its front, the others
+// at its back). Each warp takes kScanPer runs of 32 consecutive cells, a lane
 // per cell, so every load and store of a run is one coalesced line; shuffles
 // scan within the warp, warp 0 scans the warps' totals, and one atomic per
-// block reserves its work-list entries.
+// block and class reserves its work-list entries.
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 16;  // runs of 32 cells per warp: 16,384 cells per pass
 
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     const uint32_t b = blockIdx.x;
     if (b >= a.nboxes || !(rebuilding(a, b) || a.glob->grid_every_step)) return;
     const Box& bx = a.boxes[b];
-    __shared__ uint32_t s_sum[kScanThreads / 32], s_nz[kScanThreads / 32];
+    __shared__ uint32_t s_sum[kScanThreads / 32], s_nd[kScanThreads / 32], s_ns[kScanThreads / 32];
     __shared__ uint32_t s_carry, s_tile;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
@@ -149,8 +150,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     for (uint32_t tile = 0; tile < total; tile += (uint32_t)kScanThreads * kScanPer) {
         const uint32_t first = tile + warp * 32u * (uint32_t)kScanPer;
         uint32_t excl[kScanPer];  // within the warp's cells, before this lane's
-        uint32_t nonempty = 0;    // bit r: this lane's cell of run r holds particles
-        uint32_t sum = 0, nz = 0;
+        uint32_t dense = 0;       // bit r: this lane's cell of run r holds kDenseCell or more
+        uint32_t sparse = 0;      // bit r: it holds fewer, but some
+        uint32_t sum = 0, nd = 0, ns = 0;
 #pragma unroll
         for (int r = 0; r < kScanPer; r++) {
             const uint32_t c = first + 32u * (uint32_t)r + lane;
@@ -163,38 +165,47 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
             }
             excl[r] = sum + x - v;
             sum += __shfl_sync(0xffffffffu, x, 31);
-            const unsigned m = __ballot_sync(0xffffffffu, v != 0u);
-            nonempty |= (v != 0u ? 1u : 0u) << r;
-            nz += (uint32_t)__popc(m);
+            const bool d = v >= kDenseCell, sp = v != 0u && v < kDenseCell;
+            dense |= (d ? 1u : 0u) << r;
+            sparse |= (sp ? 1u : 0u) << r;
+            nd += (uint32_t)__popc(__ballot_sync(0xffffffffu, d));
+            ns += (uint32_t)__popc(__ballot_sync(0xffffffffu, sp));
         }
         if (lane == 0) {
             s_sum[warp] = sum;
-            s_nz[warp] = nz;
+            s_nd[warp] = nd;
+            s_ns[warp] = ns;
         }
         __syncthreads();
         if (warp == 0) {
-            const uint32_t ws = s_sum[lane], wn = s_nz[lane];
-            uint32_t is = ws, in = wn;
+            const uint32_t ws = s_sum[lane], wd = s_nd[lane], wp = s_ns[lane];
+            uint32_t is = ws, id = wd, ip = wp;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t ts = __shfl_up_sync(0xffffffffu, is, o);
-                const uint32_t tn = __shfl_up_sync(0xffffffffu, in, o);
+                const uint32_t td = __shfl_up_sync(0xffffffffu, id, o);
+                const uint32_t tp = __shfl_up_sync(0xffffffffu, ip, o);
                 if (lane >= (uint32_t)o) {
                     is += ts;
-                    in += tn;
+                    id += td;
+                    ip += tp;
                 }
             }
-            const uint32_t block_nz = __shfl_sync(0xffffffffu, in, 31);
-            uint32_t at = 0;
-            if (lane == 0 && block_nz) at = atomicAdd(&a.glob->work_cells, block_nz);
-            at = __shfl_sync(0xffffffffu, at, 0);
+            const uint32_t block_d = __shfl_sync(0xffffffffu, id, 31);
+            const uint32_t block_p = __shfl_sync(0xffffffffu, ip, 31);
+            uint32_t at_d = 0, at_p = 0;
+            if (lane == 0 && block_d) at_d = atomicAdd(&a.glob->work_front, block_d);
+            if (lane == 0 && block_p) at_p = atomicAdd(&a.glob->work_back, block_p);
+            at_d = __shfl_sync(0xffffffffu, at_d, 0);
+            at_p = __shfl_sync(0xffffffffu, at_p, 0);
             s_sum[lane] = is - ws;
-            s_nz[lane] = at + in - wn;
+            s_nd[lane] = at_d + id - wd;
+            s_ns[lane] = at_p + ip - wp;
             if (lane == 31u) s_tile = is;
         }
         __syncthreads();
         const uint32_t before = s_carry + s_sum[warp];
-        uint32_t at = s_nz[warp];
+        uint32_t at_d = s_nd[warp], at_p = s_ns[warp];
 #pragma unroll
         for (int r = 0; r < kScanPer; r++) {
             const uint32_t c = first + 32u * (uint32_t)r + lane;
@@ -202,10 +213,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
                 a.cell_start[base + c] = before + excl[r];
                 a.count[base + c] = 0u;
             }
-            const bool keep = (nonempty >> r) & 1u;
-            const unsigned m = __ballot_sync(0xffffffffu, keep);
-            if (keep) a.work[at + (uint32_t)__popc(m & below)] = base + c;
-            at += (uint32_t)__popc(m);
+            // dense cells from the front of the work list, the others from
+            // its back
+            const bool d = (dense >> r) & 1u, sp = (sparse >> r) & 1u;
+            const unsigned md = __ballot_sync(0xffffffffu, d);
+            const unsigned mp = __ballot_sync(0xffffffffu, sp);
+            if (d) a.work[at_d + (uint32_t)__popc(md & below)] = base + c;
+            if (sp) a.work[a.ncells - 1u - (at_p + (uint32_t)__popc(mp & below))] = base + c;
+            at_d += (uint32_t)__popc(md);
+            at_p += (uint32_t)__popc(mp);
         }
         __syncthreads();
         if (threadIdx.x == 0) s_carry += s_tile;
@@ -247,9 +263,9 @@ __global__ void sort_kernel(Arena a) {
     if (!grid_pass(a)) return;
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t cells = a.glob->work_cells;
+    const uint32_t cells = work_total(a), front = a.glob->work_front;
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cells; w += warps) {
-        const uint32_t cell = a.work[w];
+        const uint32_t cell = work_item(a, front, w);
         const uint32_t b = box_of_cell(a, cell);
         const bool reorder = a.ctrl[b].reorder != 0u;
         const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];

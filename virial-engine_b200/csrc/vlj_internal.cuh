@@ -68,6 +68,7 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #define VLJ_GATHER_AHEAD 0
 #endif
 constexpr int kForceThreads = 128;
+constexpr uint32_t kDenseCell = 8;  // particles in a cell the list build takes first
 constexpr int kTileRows = VLJ_TILE_ROWS;
 constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block
 // measurement slots: 0 kinetic, 1 potential, 2 virial, 3-5 momentum,
@@ -131,13 +132,13 @@ struct Global {
     unsigned long long step;     // steps taken: the counter of the noise stream
     unsigned long long kernels;  // kernels of this arena that ran
     uint32_t grid_every_step;    // 1: bin, scan, scatter and sort every step (one box)
-    uint32_t work_cells;         // entries of Arena::work this step
+    uint32_t work_front;         // Arena::work entries at its front: cells of kDenseCell or more
+    uint32_t work_back;          // entries at its back (work[ncells - 1 - k]): the other non-empty cells
     uint32_t next_build;         // next work entry the list build takes
     uint32_t blocks_done;        // step-kernel blocks finished (the last one decides)
     uint32_t rb_boxes;           // boxes that rebuild this step (Arena::rb_box)
     uint32_t rb_slots;           // their particles, in all
     uint32_t heat_next;          // heat-current samples written to the series so far
-    uint32_t pad;
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).
@@ -198,8 +199,10 @@ struct Arena {
     uint32_t* sorted;
     uint32_t* cell_start;  // ncells + 1
     uint32_t* count;
-    // the non-empty cells of the boxes that rebuild this step, in no set
-    // order (the scan appends them; the sort and the list build take them)
+    // the non-empty cells of the boxes that rebuild this step (ncells
+    // entries of room): those of kDenseCell particles or more from the front,
+    // the others from the back, so the list build takes the costly cells
+    // first and ends on cheap ones (work_item below)
     uint32_t* work;
     // the boxes that rebuild this step (rb_boxes of them, ascending) and the
     // running count of their particles before each (rb_first[rb_boxes] =
