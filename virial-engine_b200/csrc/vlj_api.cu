@@ -846,7 +846,8 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
         cap = std::max(cap, b.capacity);
     }
     if (slots >= (1ull << 30)) return fail(VLJ_INVALID_ARG, "at most 2^30 - 1 particles in all");
-    if (cells >= (1ull << 32) - 1) return fail(VLJ_INVALID_ARG, "too many cells in all boxes");
+    // work-list entries are cell * 8 + part
+    if (cells >= (1ull << 29)) return fail(VLJ_INVALID_ARG, "too many cells in all boxes");
     if (batched)
         s->replicas = boxes;
     else
@@ -889,7 +890,17 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.sorted, seg));
     TRY(dalloc(s, &a.cell_start, (size_t)a.ncells + 1));
     TRY(dalloc(s, &a.count, a.ncells));
-    TRY(dalloc(s, &a.work, a.ncells));
+    {
+        // room for every part of every cell: kMaxParts per cell of a narrow box
+        size_t cap = 0;
+        for (const Box& b : boxes) {
+            const bool narrow = b.cells[0] < 5u || b.cells[1] < 5u || b.cells[2] < 5u;
+            cap += (size_t)b.total_cells * (narrow ? kMaxParts : 1u);
+        }
+        if (cap >= (1ull << 32)) return fail(VLJ_INVALID_ARG, "too many cells in all boxes");
+        a.work_cap = (uint32_t)cap;
+        TRY(dalloc(s, &a.work, cap));
+    }
     TRY(dalloc(s, &a.rb_box, boxes.size()));
     TRY(dalloc(s, &a.rb_first, boxes.size() + 1));
     TRY(dalloc(s, &a.list_count, seg));

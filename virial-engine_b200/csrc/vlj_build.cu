@@ -103,18 +103,25 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    // Warps take home cells from the step's work list (the non-empty cells of
-    // the boxes that rebuild) until it runs out.
+    // Warps take home cells (or, in narrow boxes, parts of their home
+    // particles) from the step's work list (the non-empty cells of the boxes
+    // that rebuild) until it runs out.
     const uint32_t cells = work_total(a), front = a.glob->work_front;
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(&a.glob->next_build, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= cells) break;
-        const uint32_t cell = work_item(a, front, t);
+        const uint32_t entry = work_item(a, front, t);
+        const uint32_t cell = entry >> 3, part = entry & 7u;
         const uint32_t b = box_of_cell(a, cell);
-        const uint32_t hbeg = a.cell_start[cell], hend = a.cell_start[cell + 1];
         const Box& bx = a.boxes[b];
+        // this entry's home particles: the whole cell, or part `part` of it
+        // (kPartHomes each, the last part the rest)
+        const uint32_t cs0 = a.cell_start[cell], cs1 = a.cell_start[cell + 1];
+        const uint32_t parts = cell_parts(cs1 - cs0, narrow_box(bx));
+        const uint32_t hbeg = parts > 1u ? cs0 + part * kPartHomes : cs0;
+        const uint32_t hend = parts > 1u && part + 1u < parts ? hbeg + kPartHomes : cs1;
         const uint4* __restrict__ cur = a.cache[a.glob->phase];
         const float dec[3] = {bx.dec[0], bx.dec[1], bx.dec[2]};
         const int32_t n[3] = {(int32_t)bx.cells[0], (int32_t)bx.cells[1], (int32_t)bx.cells[2]};

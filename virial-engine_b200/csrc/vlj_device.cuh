@@ -42,7 +42,19 @@ __device__ __forceinline__ uint32_t work_total(const Arena& a) {
 }
 
 __device__ __forceinline__ uint32_t work_item(const Arena& a, uint32_t front, uint32_t t) {
-    return t < front ? a.work[t] : a.work[a.ncells - 1u - (t - front)];
+    return t < front ? a.work[t] : a.work[a.work_cap - 1u - (t - front)];
+}
+
+// A box under five cells wide on some axis: the list build tests on encoded
+// words there, and splits each cell's home particles into parts.
+__device__ __forceinline__ bool narrow_box(const Box& bx) {
+    return bx.cells[0] < 5u || bx.cells[1] < 5u || bx.cells[2] < 5u;
+}
+
+// Work-list entries of a cell of m particles.
+__device__ __forceinline__ uint32_t cell_parts(uint32_t m, bool narrow) {
+    if (m == 0u) return 0u;
+    return narrow ? min(kMaxParts, (m + kPartHomes - 1u) / kPartHomes) : 1u;
 }
 
 // Whether the cell grid is rebuilt this step: with the lists, or on every

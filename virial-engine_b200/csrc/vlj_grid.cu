@@ -147,14 +147,22 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
     if (threadIdx.x == 0) s_carry = bx.first;
     __syncthreads();
     const uint32_t total = bx.total_cells, base = bx.cell_base;
+    const bool narrow = narrow_box(bx);
     for (uint32_t tile = 0; tile < total; tile += (uint32_t)kScanThreads * kScanPer) {
         const uint32_t first = tile + warp * 32u * (uint32_t)kScanPer;
         uint32_t excl[kScanPer];  // within the warp's cells, before this lane's
-        uint32_t dense = 0;       // bit r: this lane's cell of run r holds kDenseCell or more
-        uint32_t sparse = 0;      // bit r: it holds fewer, but some
+        // nibble r: front entries of this lane's cell of run r (its parts,
+        // when it holds kDenseCell particles or more or the box is narrow)
+        unsigned long long front_parts = 0ull;
+        uint32_t sparse = 0;      // bit r: one back entry (a cell of fewer, but some)
         uint32_t sum = 0, nd = 0, ns = 0;
+        // the runs that reach into the box (warp-uniform; a small box has
+        // fewer cells than one pass covers)
+        const uint32_t runs = first >= total ? 0u : min((uint32_t)kScanPer, (total - first + 31u) / 32u);
 #pragma unroll
         for (int r = 0; r < kScanPer; r++) {
+            excl[r] = 0u;
+            if ((uint32_t)r >= runs) continue;
             const uint32_t c = first + 32u * (uint32_t)r + lane;
             const uint32_t v = c < total ? a.count[base + c] : 0u;
             uint32_t x = v;
@@ -165,11 +173,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
             }
             excl[r] = sum + x - v;
             sum += __shfl_sync(0xffffffffu, x, 31);
-            const bool d = v >= kDenseCell, sp = v != 0u && v < kDenseCell;
-            dense |= (d ? 1u : 0u) << r;
-            sparse |= (sp ? 1u : 0u) << r;
-            nd += (uint32_t)__popc(__ballot_sync(0xffffffffu, d));
-            ns += (uint32_t)__popc(__ballot_sync(0xffffffffu, sp));
+            if (narrow) {
+                // every non-empty cell's parts go to the front
+                const uint32_t parts = cell_parts(v, true);
+                front_parts |= (unsigned long long)parts << (4 * r);
+                nd += __reduce_add_sync(0xffffffffu, parts);
+            } else {
+                const bool d = v >= kDenseCell, sp = v != 0u && v < kDenseCell;
+                front_parts |= (unsigned long long)(d ? 1u : 0u) << (4 * r);
+                sparse |= (sp ? 1u : 0u) << r;
+                nd += (uint32_t)__popc(__ballot_sync(0xffffffffu, d));
+                ns += (uint32_t)__popc(__ballot_sync(0xffffffffu, sp));
+            }
         }
         if (lane == 0) {
             s_sum[warp] = sum;
@@ -208,19 +223,34 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
         uint32_t at_d = s_nd[warp], at_p = s_ns[warp];
 #pragma unroll
         for (int r = 0; r < kScanPer; r++) {
+            if ((uint32_t)r >= runs) continue;
             const uint32_t c = first + 32u * (uint32_t)r + lane;
             if (c < total) {
                 a.cell_start[base + c] = before + excl[r];
                 a.count[base + c] = 0u;
             }
-            // dense cells from the front of the work list, the others from
-            // its back
-            const bool d = (dense >> r) & 1u, sp = (sparse >> r) & 1u;
-            const unsigned md = __ballot_sync(0xffffffffu, d);
+            // costly cells' parts from the front of the work list, the
+            // others from its back
+            const uint32_t kd = (uint32_t)(front_parts >> (4 * r)) & 15u;
+            if (narrow) {
+                // several parts a cell: an exclusive scan of the counts
+                uint32_t incl = kd;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (uint32_t)o) incl += t;
+                }
+                for (uint32_t q = 0; q < kd; q++) a.work[at_d + incl - kd + q] = (base + c) * 8u + q;
+                at_d += __shfl_sync(0xffffffffu, incl, 31);
+            } else {
+                // one entry at most: a ballot ranks them
+                const unsigned md = __ballot_sync(0xffffffffu, kd != 0u);
+                if (kd) a.work[at_d + (uint32_t)__popc(md & below)] = (base + c) * 8u;
+                at_d += (uint32_t)__popc(md);
+            }
+            const bool sp = (sparse >> r) & 1u;
             const unsigned mp = __ballot_sync(0xffffffffu, sp);
-            if (d) a.work[at_d + (uint32_t)__popc(md & below)] = base + c;
-            if (sp) a.work[a.ncells - 1u - (at_p + (uint32_t)__popc(mp & below))] = base + c;
-            at_d += (uint32_t)__popc(md);
+            if (sp) a.work[a.work_cap - 1u - (at_p + (uint32_t)__popc(mp & below))] = (base + c) * 8u;
             at_p += (uint32_t)__popc(mp);
         }
         __syncthreads();
@@ -265,7 +295,9 @@ __global__ void sort_kernel(Arena a) {
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t cells = work_total(a), front = a.glob->work_front;
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cells; w += warps) {
-        const uint32_t cell = work_item(a, front, w);
+        const uint32_t entry = work_item(a, front, w);
+        if (entry & 7u) continue;  // a cell sorts once, with its first part
+        const uint32_t cell = entry >> 3;
         const uint32_t b = box_of_cell(a, cell);
         const bool reorder = a.ctrl[b].reorder != 0u;
         const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];

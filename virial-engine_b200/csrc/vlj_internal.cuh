@@ -69,6 +69,13 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #endif
 constexpr int kForceThreads = 128;
 constexpr uint32_t kDenseCell = 8;  // particles in a cell the list build takes first
+// In a box under five cells wide on some axis (a batched replica) a cell
+// holds many particles and its candidate stream is most of the box, so its
+// home particles split into parts of kPartHomes (at most kMaxParts, the
+// last taking the rest), each a work-list entry of its own: entry = cell * 8
+// + part.
+constexpr uint32_t kPartHomes = 8;
+constexpr uint32_t kMaxParts = 8;
 constexpr int kTileRows = VLJ_TILE_ROWS;
 constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block
 // measurement slots: 0 kinetic, 1 potential, 2 virial, 3-5 momentum,
@@ -199,11 +206,13 @@ struct Arena {
     uint32_t* sorted;
     uint32_t* cell_start;  // ncells + 1
     uint32_t* count;
-    // the non-empty cells of the boxes that rebuild this step (ncells
-    // entries of room): those of kDenseCell particles or more from the front,
-    // the others from the back, so the list build takes the costly cells
-    // first and ends on cheap ones (work_item below)
+    // the non-empty cells of the boxes that rebuild this step, as entries
+    // cell * 8 + part (one part per cell but in narrow boxes): those of
+    // kDenseCell particles or more and every part of a narrow box's cell
+    // from the front, the others from the back, so the list build takes the
+    // costly work first and ends on cheap work (work_item below)
     uint32_t* work;
+    uint32_t work_cap;   // entries of room in work
     // the boxes that rebuild this step (rb_boxes of them, ascending) and the
     // running count of their particles before each (rb_first[rb_boxes] =
     // rb_slots): the per-particle rebuild kernels cover only these
