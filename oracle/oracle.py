@@ -112,6 +112,10 @@ _sig("vo_md_read", None, [C.c_void_p, _dp, _dp])
 _sig("vo_md_set_heat_exchange", None, [C.c_void_p, C.c_int, _dp, C.c_double])
 _sig("vo_md_set_threads", None, [C.c_int])
 _sig("vo_md_threads", C.c_int, [])
+_sig("vo_dfmd_create", C.c_void_p, [_dp, _dp, C.c_uint32, _dp, C.c_double, C.c_int, C.c_double])
+_sig("vo_dfmd_run", None, [C.c_void_p, C.c_uint64])
+_sig("vo_dfmd_measure", None, [C.c_void_p, _dp, C.c_void_p, C.c_void_p])
+_sig("vo_dfmd_destroy", None, [C.c_void_p])
 
 
 def _f64(a):
@@ -313,6 +317,40 @@ class MD:
     def close(self):
         if self._h:
             _lib.vo_md_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class DoubleFloatMD:
+    """The reference's plain double-float path at constant energy
+    (double-float state, f32 pair arithmetic on packed positions, df64 sums;
+    dfpath.c), for the error table against the f64 truth."""
+
+    def __init__(self, pos, vel, box, cutoff=2.5, dt=0.005, shifted_force=False):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        self._h = _lib.vo_dfmd_create(pos, vel, len(pos), _f64(box), cutoff, int(shifted_force), dt)
+        if not self._h:
+            raise ValueError("the box must be at least three cutoffs wide on every axis")
+        self.n = len(pos)
+
+    def run(self, steps):
+        _lib.vo_dfmd_run(self._h, steps)
+
+    def measure(self):
+        """(kinetic, potential, virial, positions, velocities)"""
+        out = np.zeros(3)
+        pos = np.zeros((self.n, 3))
+        vel = np.zeros((self.n, 3))
+        _lib.vo_dfmd_measure(self._h, out, pos.ctypes.data_as(C.c_void_p),
+                             vel.ctypes.data_as(C.c_void_p))
+        return out[0], out[1], out[2], pos, vel
+
+    def close(self):
+        if self._h:
+            _lib.vo_dfmd_destroy(self._h)
             self._h = None
 
     def __del__(self):

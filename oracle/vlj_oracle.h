@@ -162,6 +162,19 @@ void vo_md_set_heat_exchange(vo_md *md, int on, const double slabs[4], double en
 void vo_md_set_threads(int threads);
 int vo_md_threads(void);
 
+
+/* The reference's plain double-float path (dfpath.c), constant energy:
+ * double-float state, f32 pair arithmetic on packed positions, df64 sums.
+ * NULL when the box is under three cutoffs wide on some axis. measure gives
+ * kinetic, potential and virial, and the state as f64 into pos / vel (either
+ * may be NULL). */
+typedef struct vo_dfmd vo_dfmd;
+vo_dfmd *vo_dfmd_create(const double *pos, const double *vel, uint32_t n, const double box[3],
+                        double cutoff, int shifted_force, double dt);
+void vo_dfmd_run(vo_dfmd *m, uint64_t steps);
+void vo_dfmd_measure(vo_dfmd *m, double out[3], double *pos, double *vel);
+void vo_dfmd_destroy(vo_dfmd *m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,3 +142,30 @@ def test_second_virial_coefficient():
     # (docs/VALIDATION.md:45 quotes the reference's measurement against it)
     b2 = second_virial(2.0, 2.5)
     assert abs(1.0 + b2 * 0.01 - 0.99228) < 2e-5
+
+
+def test_double_float_path_meets_the_reference_bound(O):
+    # The reference's own arithmetic (dfpath.c) on the small plain workload:
+    # PE and virial within the 1e-5 its tests allow against f64 pairs
+    # (tests/thermodynamics.rs:93-97); over 100 constant-energy steps its
+    # energy moves as the f64 engine's does (the change from the lattice start
+    # is the integrator's, not the arithmetic's).
+    L = (1000 / 0.8442) ** (1.0 / 3.0)
+    pos, vel = O.lattice(1000, L, 0.72, 1)
+    box = np.array([float(np.float32(L))] * 3)
+    md = O.DoubleFloatMD(pos, vel, box, 2.5, 0.005, False)
+    ke, pe, w, p, _ = md.measure()
+    pe64, w64 = O.all_pairs(np.mod(p, box), box, 2.5, False)
+    assert abs((pe - pe64) / pe64) < 1e-5 and abs((w - w64.sum()) / w64.sum()) < 1e-5
+    md.run(100)
+    ke1, pe1, _, _, _ = md.measure()
+    f64 = O.MD(pos, vel, box, cutoff=2.5, skin=0.3, dt=0.005)
+    m0 = f64.measure()
+    f64.run(100)
+    m1 = f64.measure()
+    e0 = m0.kinetic + m0.potential
+    change = ((ke1 + pe1) - (ke + pe)) / abs(ke + pe)
+    change64 = ((m1.kinetic + m1.potential) - e0) / abs(e0)
+    assert abs(change - change64) < 1e-5, (change, change64)
+    with pytest.raises(ValueError):
+        O.DoubleFloatMD(pos, vel, [7.0, 7.0, 7.0], 2.5, 0.005, False)
