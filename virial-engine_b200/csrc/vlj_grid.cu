@@ -126,8 +126,10 @@ __global__ void bin_kernel(Arena a) {
 // ---- scan (grid.wgsl:43-117): one block per box, exclusive prefix sum of
 // the counts offset by the box's first slot; counts become zeroed cursors.
 // The box's non-empty cells join the step's work list for the sort and the
-// list build (cells of kDenseCell particles or more at its front, the others
-// at its back). Each warp takes kScanPer runs of 32 consecutive cells, a lane
+// list build as entries cell * 8 + part: cells of kDenseCell particles or
+// more at its front, the others at its back; in a narrow box every non-empty
+// cell's parts (kPartHomes home particles each) at its front. Each warp takes
+// kScanPer runs of 32 consecutive cells, a lane
 // per cell, so every load and store of a run is one coalesced line; shuffles
 // scan within the warp, warp 0 scans the warps' totals, and one atomic per
 // block and class reserves its work-list entries.
