@@ -1087,13 +1087,13 @@ static vlj_status step_direct(vlj_sim* s, bool heat = false) {
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
     if (steps > 0 && s->heat_pending) {
         // the first step's force pass takes the requested heat-current sample
-        s->heat_pending = false;
         if (s->timing || !s->use_graphs) {
             TRY(step_direct(s, true));
         } else {
             if (!s->graph_one_heat) TRY(build_graph(s, 1, &s->graph_one_heat, true));
             CUDA_TRY(cudaGraphLaunch(s->graph_one_heat, s->stream));
         }
+        s->heat_pending = false;
         steps -= 1;
     }
     if (s->timing || !s->use_graphs) {
