@@ -152,6 +152,18 @@ struct Profile {
         }
         return out;
     }
+    // Mean of a per-slab quantity over the slabs in `phase` (lennard_jones.rs:262-271);
+    // empty when there are none.
+    std::optional<double> mean_in(const std::vector<double>& values,
+                                  const std::vector<Phase>& phases, Phase phase) const {
+        double sum = 0.0, n = 0.0;
+        for (size_t k = 0; k < values.size() && k < phases.size(); k++)
+            if (phases[k] == phase) {
+                sum += values[k];
+                n += 1.0;
+            }
+        return n > 0.0 ? std::optional<double>(sum / n) : std::nullopt;
+    }
     double surface_tension() const {
         const auto p = total_pressure_tensor();
         return 0.5 * box_size[2] * (p[2] - 0.5 * (p[0] + p[1]));

@@ -197,10 +197,15 @@ void phases_of_two_slabs_across_the_boundary() {
     auto count = [&](Phase q) { return std::count(phases.begin(), phases.end(), q); };
     EXPECT(count(Phase::Liquid) == 6 + 6 + 7, "%ld", (long)count(Phase::Liquid));
     EXPECT(count(Phase::Interface) == 16, "%ld", (long)count(Phase::Interface));
+    const auto density = p.density();
+    EXPECT(std::fabs(*p.mean_in(density, phases, Phase::Liquid) - 0.7) < 1e-12, "liquid mean");
+    EXPECT(std::fabs(*p.mean_in(density, phases, Phase::Vapour) - 0.02) < 1e-12, "vapour mean");
     Profile flat;
     flat.box_size = {1.0, 1.0, 8.0};
     for (int b = 0; b < 8; b++) flat.slabs.push_back({b + 0.5, 0.3, {}, {}, 0.0});
-    for (Phase q : flat.phases(0.36, 4.0)) EXPECT(q == Phase::Between, "flat profile");
+    const auto flat_phases = flat.phases(0.36, 4.0);
+    for (Phase q : flat_phases) EXPECT(q == Phase::Between, "flat profile");
+    EXPECT(!flat.mean_in(flat.density(), flat_phases, Phase::Liquid), "no liquid slab");
 }
 
 void no_device_is_an_error() {
