@@ -315,6 +315,65 @@ void thermostatted_reruns_are_bit_identical() {
     EXPECT(once() == once(), "states or measurements differ between runs");
 }
 
+// Least-squares rate of energy against time and its standard error
+// (tests/heat.rs:141-157).
+std::pair<double, double> drift(const std::vector<double>& t, const std::vector<double>& e) {
+    const double n = (double)t.size();
+    double mt = 0.0, me = 0.0;
+    for (size_t k = 0; k < t.size(); k++) {
+        mt += t[k] / n;
+        me += e[k] / n;
+    }
+    double sxx = 0.0, sxy = 0.0;
+    for (size_t k = 0; k < t.size(); k++) {
+        sxx += (t[k] - mt) * (t[k] - mt);
+        sxy += (t[k] - mt) * (e[k] - me);
+    }
+    const double rate = sxy / sxx;
+    double residual = 0.0;
+    for (size_t k = 0; k < t.size(); k++) {
+        const double r = e[k] - me - rate * (t[k] - mt);
+        residual += r * r;
+    }
+    return {rate, std::sqrt(residual / (n - 2.0) / sxx)};
+}
+
+void heat_exchange_moves_energy_and_keeps_momentum() {
+    // tests/heat.rs:159-214
+    const std::array<double, 3> size = {9.0, 9.0, 36.0};
+    const double dt = 0.002;
+    const size_t count = (size_t)std::lround(0.8442 * size[0] * size[1] * size[2]);
+    Settings s;
+    s.box_size = size;
+    s.dt = dt;
+    s.shifted_force = true;
+    s.profile_bins = 12;
+    LennardJones sim(lattice_box(count, size, 1.0, 11), s);
+    sim.run(2000);
+    const Measurement before = sim.measure_now();
+    const double energy = 0.01;
+    sim.set_heat_exchange(HeatExchange{{0.0, 3.0}, {18.0, 21.0}, energy});
+    std::vector<double> time, total;
+    for (int k = 0; k < 200; k++) {
+        sim.run(100);
+        sim.sample_profile_now();
+        const Measurement m = sim.measure_now();
+        time.push_back(m.time);
+        total.push_back(m.energy());
+    }
+    const Measurement after = sim.measure_now();
+    const auto [rate, error] = drift(time, total);
+    const double duration = time.back() - time.front();
+    const double moved = energy / dt * duration;
+    const auto t = sim.read_profile().temperature();
+    EXPECT(std::fabs(rate * duration) < 1e-3 * moved, "energy not conserved: %g +/- %g", rate,
+           error);
+    for (int k = 0; k < 3; k++)
+        EXPECT(std::fabs(after.momentum[k] - before.momentum[k]) < 1e-6 * after.count,
+               "momentum changed: %g", after.momentum[k] - before.momentum[k]);
+    EXPECT(t[0] > t[6] + 0.04, "hot slab %.4f not hotter than cold slab %.4f", t[0], t[6]);
+}
+
 void measurements_arrive_in_order() {
     // lennard_jones.rs:1141-1163, 1194-1260: measure enqueues, poll returns
     // finished measurements oldest first; measure_now equals a polled one
@@ -401,6 +460,8 @@ int main(int argc, char** argv) {
         run("rectangular_box_matches_all_pairs", rectangular_box_matches_all_pairs);
         run("profiles_add_up_to_the_whole_box", profiles_add_up_to_the_whole_box);
         run("thermostatted_reruns_are_bit_identical", thermostatted_reruns_are_bit_identical);
+        run("heat_exchange_moves_energy_and_keeps_momentum",
+            heat_exchange_moves_energy_and_keeps_momentum);
         run("measurements_arrive_in_order", measurements_arrive_in_order);
         run("panics_become_errors", panics_become_errors);
     }

@@ -39,5 +39,6 @@ def test_cpp_mirror_reference_tests(gpu, tmp_path):
     out = run(build(gpu, str(tmp_path)), "gpu", 600)
     for name in ["cell_grid_finds_every_pair", "rectangular_box_matches_all_pairs",
                  "profiles_add_up_to_the_whole_box", "thermostatted_reruns_are_bit_identical",
+                 "heat_exchange_moves_energy_and_keeps_momentum",
                  "measurements_arrive_in_order", "panics_become_errors"]:
         assert "ok   " + name in out
