@@ -169,3 +169,18 @@ def test_double_float_path_meets_the_reference_bound(O):
     assert abs(change - change64) < 1e-5, (change, change64)
     with pytest.raises(ValueError):
         O.DoubleFloatMD(pos, vel, [7.0, 7.0, 7.0], 2.5, 0.005, False)
+
+
+@pytest.mark.parametrize("shifted_force", [False, True])
+def test_double_float_path_in_the_liquid(O, shifted_force):
+    # after 200 steps from the lattice (a liquid): the reference's arithmetic
+    # stays within its own 1e-5 of the f64 pair sums in both cutoff styles
+    L = (1000 / 0.8442) ** (1.0 / 3.0)
+    pos, vel = O.lattice(1000, L, 0.72, 1)
+    box = np.array([float(np.float32(L))] * 3)
+    md = O.DoubleFloatMD(pos, vel, box, 2.5, 0.005, shifted_force)
+    md.run(200)
+    ke, pe, w, p, v = md.measure()
+    pe64, w64 = O.all_pairs(np.mod(p, box), box, 2.5, shifted_force)
+    assert abs((pe - pe64) / pe64) < 1e-5 and abs((w - w64.sum()) / w64.sum()) < 1e-5
+    assert abs(ke - 0.5 * np.sum(v * v)) < 1e-9 * ke
