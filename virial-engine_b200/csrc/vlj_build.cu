@@ -34,13 +34,23 @@
 
 namespace vlj {
 
-constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
-constexpr int kRound = 128;     // candidates a warp fetches per round
-constexpr int kStage = 512;     // staged candidates a warp holds (a dense cell's all)
+// Tuning knobs of the list build (tune.py --kernel build sweeps them): the
+// candidates a warp fetches per round, the staged candidates it holds (a
+// dense cell's all), and the resident blocks per SM its registers are sized for.
+#ifndef VLJ_BUILD_ROUND
+#define VLJ_BUILD_ROUND 128
+#endif
+#ifndef VLJ_BUILD_STAGE
+#define VLJ_BUILD_STAGE 512
+#endif
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
 #endif
-constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;  // register budget of the build
+constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
+constexpr int kRound = VLJ_BUILD_ROUND;
+constexpr int kStage = VLJ_BUILD_STAGE;
+constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;
+static_assert(kRound % 32 == 0 && kStage % 32 == 0 && kRound <= kStage, "build stage shape");
 
 // The reference's packed position of slot s: the f32 hi part of each f64
 // coordinate and the f32 lo part of the rest (Df64::from_f64,

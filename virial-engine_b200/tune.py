@@ -12,6 +12,12 @@ L2 flushed between steps), and prints the ranking as JSON lines. Needs a GPU.
 
 The winner's settings become the defaults of VLJ_LIST_STREAM / VLJ_L1_CARVEOUT
 (csrc/vlj_internal.cuh, csrc/vlj_forces.cu) or VLJ_TILE_ROWS / VLJ_TILE_SLOTS.
+
+    python virial-engine_b200/tune.py --kernel build [--cells 40] [--steps 30]
+
+times the list build's variants instead (candidates per round, staged
+candidates per warp, blocks per SM: VLJ_BUILD_* in csrc/vlj_build.cu) by the
+wall time of a forced rebuild.
 """
 
 import argparse
@@ -25,6 +31,14 @@ OUT_DIR = os.path.join(HERE, "build", "tune")
 # name -> preprocessor overrides: rows streamed without L1 allocation under
 # shared-memory carve-out hints (percent), or the TMA tile ring (rows per tile,
 # tiles in flight)
+# list-build variants: candidates fetched per round, staged per warp, and the
+# blocks per SM the registers are sized for
+BUILD_CANDIDATES = {
+    "round128_stage512_b6": {},
+    "round64_stage512_b6": {"VLJ_BUILD_ROUND": 64},
+    "round128_stage384_b6": {"VLJ_BUILD_STAGE": 384},
+    "round128_stage512_b5": {"VLJ_BUILD_BLOCKS_PER_SM": 5},
+}
 CANDIDATES = {
     "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
     "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
@@ -57,30 +71,57 @@ def child(lib, cells, steps):
     print(json.dumps({"step_kernel_us": ms * 1e3 / n, "launches": n}))
 
 
+def build_child(lib, cells, rebuilds):
+    """Wall time of a forced rebuild (decide, the grid, the list build; the
+    stream waited on), averaged: the list build is most of it."""
+    os.environ["VLJ_LIBRARY"] = lib
+    sys.path.insert(0, HERE)
+    import time
+    import virial_lj as vl
+    p, box = vl.lattice_fcc(cells, 0.8442, 1.0, 7)
+    sim = vl.LennardJones(p, vl.Settings([box] * 3, dt=0.005, shifted_force=True,
+                                         thermostat=vl.Langevin(1.0, 1.0, 7)))
+    sim.run(20)
+    sim.force_rebuild()
+    t0 = time.perf_counter()
+    for _ in range(rebuilds):
+        sim.force_rebuild()
+    us = (time.perf_counter() - t0) / rebuilds * 1e6
+    print(json.dumps({"rebuild_us": us, "rebuilds": rebuilds}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--child", default=None)
+    ap.add_argument("--kernel", choices=["step", "build"], default="step",
+                    help="tune the force kernels' list reading (step) or the list build")
     ap.add_argument("--no-build", action="store_true",
                     help="time the variants already in build/tune (built elsewhere)")
     ap.add_argument("--build-only", action="store_true", help="build the variants, time nothing")
     args = ap.parse_args()
     if args.child:
-        child(args.child, args.cells, args.steps)
+        if args.kernel == "build":
+            build_child(args.child, args.cells, args.steps)
+        else:
+            child(args.child, args.cells, args.steps)
         return
     sys.path.insert(0, HERE)
     import build
     os.makedirs(OUT_DIR, exist_ok=True)
     results = []
-    for name, defines in CANDIDATES.items():
+    candidates = BUILD_CANDIDATES if args.kernel == "build" else CANDIDATES
+    key = "rebuild_us" if args.kernel == "build" else "step_kernel_us"
+    for name, defines in candidates.items():
         lib = os.path.join(OUT_DIR, f"libvirial_lj_{name}.so")
         if not args.no_build:
             build.build(defines=defines, out=lib, force=True)
         if args.build_only:
             continue
         out = subprocess.run([sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
-                              "--steps", str(args.steps)], capture_output=True, text=True)
+                              "--steps", str(args.steps), "--kernel", args.kernel],
+                             capture_output=True, text=True)
         if out.returncode != 0:
             print(json.dumps({"variant": name, "error": out.stderr[-500:]}), flush=True)
             continue
@@ -89,7 +130,7 @@ def main():
         results.append(r)
         print(json.dumps(r), flush=True)
     if results:
-        best = min(results, key=lambda r: r["step_kernel_us"])
+        best = min(results, key=lambda r: r[key])
         print(json.dumps({"best": best}))
 
 
