@@ -265,12 +265,18 @@ VLJ_API vlj_status vlj_batch_box_size(const vlj_batch *batch, size_t replica, do
  * cell_of[count]. Work is enqueued on `stream` (a cudaStream_t, or NULL).
  *
  * Limits and sharing: at most VLJ_BIN_NOALLOC_MAX_CELLS cells (larger grids
- * are rejected with VLJ_INVALID_ARG). The per-cell counters live in one fixed
- * device array (VLJ_BIN_NOALLOC_MAX_CELLS x 4 bytes) that every GPU loading
- * the library holds until exit and that every call shares: calls whose work
- * overlaps on the GPU race with each other, so serialise them (one stream, or
- * events). The first call on a device looks up that array's address and
- * should come before any stream capture. */
+ * are rejected with VLJ_INVALID_ARG). Any number of particles per cell: cells
+ * of more than 32 are ordered by a block-wide sorting network, O(m log^2 m)
+ * for m particles, in shared memory up to 8192 and in place in `sorted`
+ * beyond that (correct but slow: a million particles in one cell take a
+ * sizeable fraction of a second). The per-cell counters live in one fixed
+ * device array ((VLJ_BIN_NOALLOC_MAX_CELLS + 1) x 4 bytes) that every GPU
+ * loading the library holds until exit and that every call shares: calls
+ * whose work overlaps on the GPU race with each other, so serialise them (one
+ * stream, or events). Each call looks up that array's address in the current
+ * context (so a device reset between calls is safe); the first call on a
+ * device also loads the library's device code and should come before any
+ * stream capture. */
 #define VLJ_BIN_NOALLOC_MAX_CELLS 262144u
 VLJ_API vlj_status vlj_bin_noalloc(const double *pos, size_t count, const double box_size[3],
                                    const uint32_t cells[3], uint32_t *sorted,
@@ -323,6 +329,13 @@ VLJ_API vlj_status vlj_debug_kernel_time(vlj_sim *sim, double *total_ms, uint64_
 /* FP32 FMA throughput of the current device in TFLOP/s (a calibration kernel
  * of independent FMA chains on every SM). */
 VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
+/* The Langevin noise stream as the device computes it (known-answer checks):
+ * for k < n, out[4k..4k+3] = Philox-4x32-10 of counter ctr[4k..4k+3] and key
+ * key[2k..2k+1], and noise[3k..3k+2] = the three Gaussian numbers the step
+ * kernel draws for particle id ctr[4k] at step ctr[4k+1] + 2^32 ctr[4k+2]
+ * with seed key[2k]. Host buffers; n at most 2^24; waits. */
+VLJ_API vlj_status vlj_debug_philox(const uint32_t *ctr, const uint32_t *key, size_t n,
+                                    uint32_t *out, float *noise);
 /* The simulation that steps a batch's arena, for vlj_debug_set_graphs,
  * vlj_debug_kernel_timing / _time and vlj_debug_kernels_executed only (it
  * stays owned by the batch). */

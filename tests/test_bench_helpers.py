@@ -20,7 +20,7 @@ def bench():
 
 def test_config_names_the_workload(bench):
     c = bench.config(256000, 1)
-    assert c["workload"] == "lj-fcc40x4-256k-rho0.8442-shifted-force-langevin"
+    assert c["workload"] == "lj-fcc40x4-256k-rho0.8442-shifted-force-langevin-grid-on-list-trigger"
     assert c["particles_per_box"] == 256000 and c["parallelism"] == "replicas x1"
     assert "flushed" in c["l2"] and "grid" in c
     json.dumps(c)
@@ -39,6 +39,18 @@ def test_roofline_inputs_from_committed_files(bench):
     # the step kernel's DRAM bytes per launch from its committed ncu summary:
     # well above the 96 B x 256,000 algorithmic bytes (the list streams)
     assert traffic is not None and 96 * 256000 < traffic < 1e9
+
+
+def test_roofline_picks_the_binding_roof(bench):
+    # rho 0.8442: 2,290 flop against 96 B per particle-step, above the machine
+    # balance, so the FP32 roof binds and its fraction is the headline
+    line = bench.roofline_line(500.0, 6500.0, "measured", 11.5, 71.0, 2290.0, 1e8, 51e-6, 200)
+    assert line["bound"] == "fp32" and line["unit"] == "TFLOP/s"
+    assert abs(line["frac"] - 11.5 / 71.0) < 1e-12
+    assert line["hbm"]["frac"] < line["frac"]
+    line = bench.roofline_line(3000.0, 6500.0, "measured", 1.0, 71.0, 20.0, 1e8, 51e-6, 200)
+    assert line["bound"] == "hbm" and line["unit"] == "GB/s"
+    json.dumps(line)
 
 
 def test_metric_and_unit(bench):

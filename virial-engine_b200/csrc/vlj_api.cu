@@ -769,6 +769,41 @@ vlj_status vlj_debug_fp32_peak(double* tflops) {
     return VLJ_OK;
 }
 
+vlj_status vlj_debug_philox(const uint32_t* ctr, const uint32_t* key, size_t n, uint32_t* out,
+                            float* noise) {
+    if (!ctr || !key || !out || !noise) return fail(VLJ_INVALID_ARG, "null argument");
+    if (n == 0 || n > (1u << 24)) return fail(VLJ_INVALID_ARG, "n must be in 1 .. 2^24");
+    cudaStream_t st;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    uint4 *d_ctr = nullptr, *d_out = nullptr;
+    uint2* d_key = nullptr;
+    float4* d_noise = nullptr;
+    cudaError_t e = cudaMalloc(&d_ctr, sizeof(uint4) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_key, sizeof(uint2) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(uint4) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_noise, sizeof(float4) * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ctr, ctr, sizeof(uint4) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_key, key, sizeof(uint2) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_philox_check(d_ctr, d_key, (uint32_t)n, d_out, d_noise, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(uint4) * n, cudaMemcpyDeviceToHost, st);
+    std::vector<float4> nz(e == cudaSuccess ? n : 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nz.data(), d_noise, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_ctr);
+    cudaFree(d_key);
+    cudaFree(d_out);
+    cudaFree(d_noise);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return fail(VLJ_CUDA_ERROR, "debug_philox: %s", cudaGetErrorString(e));
+    for (size_t k = 0; k < n; k++) {
+        noise[3 * k] = nz[k].x;
+        noise[3 * k + 1] = nz[k].y;
+        noise[3 * k + 2] = nz[k].z;
+    }
+    return VLJ_OK;
+}
+
 vlj_status vlj_debug_launches(uint64_t* n) {
     if (!n) return fail(VLJ_INVALID_ARG, "null argument");
     *n = launches();

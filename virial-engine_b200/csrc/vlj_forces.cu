@@ -754,6 +754,29 @@ __global__ void __launch_bounds__(kBlock) fp32_peak_kernel(float* out, int iters
     if (t == 12345.678f) out[blockIdx.x] = t;  // keeps the chains live
 }
 
+// ---- the noise stream as the step kernel draws it, for known-answer checks:
+// Philox-4x32-10 of each (counter, key), and the Langevin noise of
+// (id = ctr.x, step = ctr.y + 2^32 ctr.z, seed = key.x) ----
+__global__ void __launch_bounds__(kBlock) philox_check_kernel(const uint4* __restrict__ ctr,
+                                                              const uint2* __restrict__ key,
+                                                              uint32_t n, uint4* __restrict__ out,
+                                                              float4* __restrict__ noise) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint4 c = ctr[k];
+    const uint2 q = key[k];
+    out[k] = philox4x32_10(c, q);
+    float xi[3];
+    langevin_noise(c.x, (unsigned long long)c.y | ((unsigned long long)c.z << 32), q.x, xi);
+    noise[k] = make_float4(xi[0], xi[1], xi[2], 0.0f);
+}
+
+cudaError_t launch_philox_check(const uint4* ctr, const uint2* key, uint32_t n, uint4* out,
+                                float4* noise, cudaStream_t s) {
+    philox_check_kernel<<<blocks_for(n), kBlock, 0, s>>>(ctr, key, n, out, noise);
+    return after_launch();
+}
+
 // ---- launchers ----
 static unsigned particle_blocks(const Arena& a) {
     return blocks_for(a.nslots, kForceThreads);

@@ -294,11 +294,10 @@ __device__ __forceinline__ float nearest_ref(float d, float side) {
     return __fsub_rn(d, __fmul_rn(side, rintf(__fdiv_rn(d, side))));
 }
 
-// ---- Philox-4x32-10 (Salmon et al., SC'11), counter (id, step lo, step hi,
-// 0), key (seed, "LJV1") ----
-__device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, uint32_t seed) {
-    uint32_t c0 = id, c1 = (uint32_t)step, c2 = (uint32_t)(step >> 32), c3 = 0u;
-    uint32_t k0 = seed, k1 = 0x4C4A5631u;
+// ---- Philox-4x32-10 (Salmon et al., SC'11) of counter c and key k ----
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+    uint32_t c0 = c.x, c1 = c.y, c2 = c.z, c3 = c.w;
+    uint32_t k0 = k.x, k1 = k.y;
 #pragma unroll
     for (int r = 0; r < 10; r++) {
         uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
@@ -312,6 +311,13 @@ __device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, ui
         k1 += 0xBB67AE85u;
     }
     return make_uint4(c0, c1, c2, c3);
+}
+
+// The Langevin noise stream: counter (id, step lo, step hi, 0), key (seed,
+// "LJV1"), one Philox block per particle and step.
+__device__ __forceinline__ uint4 philox(uint32_t id, unsigned long long step, uint32_t seed) {
+    return philox4x32_10(make_uint4(id, (uint32_t)step, (uint32_t)(step >> 32), 0u),
+                         make_uint2(seed, 0x4C4A5631u));
 }
 
 // r . F and U of a pair at r2 < rc2 (lennard_jones.wgsl:533-545), for the
@@ -476,6 +482,10 @@ cudaError_t launch_drawn_temperature(const Arena& a, cudaStream_t s);
 cudaError_t launch_heat_current(const Arena& a, bool shifted_force, uint32_t sample,
                                 cudaStream_t s);
 cudaError_t launch_fp32_peak(float* out, int blocks, int iters, cudaStream_t s);
+// Philox-4x32-10 of n (counter, key) pairs and the Langevin noise the step
+// kernel draws for each (id, step, seed) read from them (vlj_debug_philox).
+cudaError_t launch_philox_check(const uint4* ctr, const uint2* key, uint32_t n, uint4* out,
+                                float4* noise, cudaStream_t s);
 unsigned long long launches();
 
 }  // namespace vlj

@@ -14,20 +14,23 @@
 // a stable counting sort, so each cell lists its particles in index order.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "virial_lj.h"
 #include "vlj_common.h"
 
 namespace vlj {
 namespace {
 
-// Per-cell counts, then fill cursors, shared by every call on a device.
-__device__ __align__(256) uint32_t g_bin_scratch[VLJ_BIN_NOALLOC_MAX_CELLS];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-uint32_t* g_scratch[kMaxDevices] = {};
+// Per-cell counts, then fill cursors, shared by every call on a device; once
+// the particles are scattered, the same words list the cells of more than 32
+// particles for the block-wide sort, and the word after the last cell counts
+// them.
+constexpr uint32_t kLargeCount = VLJ_BIN_NOALLOC_MAX_CELLS;
+__device__ __align__(256) uint32_t g_bin_scratch[VLJ_BIN_NOALLOC_MAX_CELLS + 1];
+// Cells up to this many particles are sorted in shared memory; larger ones
+// in place in global memory (same network, slower).
+constexpr uint32_t kSharedSort = 8192;
+constexpr int kSortThreads = 1024;
+constexpr unsigned kLargeBlocks = 296;  // blocks that take the listed cells in turn
 
 struct BinGrid {
     float cell_size[3];
@@ -36,22 +39,15 @@ struct BinGrid {
     uint32_t n;
 };
 
-// The device address of the scratch array on the current device, looked up
-// once per device (in host code the array's name is not a device address).
+// The device address of the scratch array in the current device's context.
+// In host code the array's name is only a stand-in for it. Looked up on every
+// call, so an address never outlives the context it belongs to (a device
+// reset creates a new one).
 vlj_status scratch_address(uint32_t** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(VLJ_CUDA_ERROR, "cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return fail(VLJ_INVALID_ARG, "device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_bin_scratch);
-        if (e != cudaSuccess)
-            return fail(VLJ_CUDA_ERROR, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_scratch[dev] = static_cast<uint32_t*>(p);
-    }
-    *out = g_scratch[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_bin_scratch);
+    if (e != cudaSuccess) return fail(VLJ_CUDA_ERROR, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    *out = static_cast<uint32_t*>(p);
     return VLJ_OK;
 }
 
@@ -110,7 +106,10 @@ __global__ void __launch_bounds__(1024) nb_scan(BinGrid g, uint32_t* __restrict_
         if (threadIdx.x == 0) s_carry += s_warp[31];
         __syncthreads();
     }
-    if (threadIdx.x == 0) cell_start[g.total] = g.n;
+    if (threadIdx.x == 0) {
+        cell_start[g.total] = g.n;
+        counts[kLargeCount] = 0u;  // no large cell listed yet
+    }
 }
 
 __global__ void nb_scatter(BinGrid g, const uint32_t* __restrict__ cell_of,
@@ -124,8 +123,10 @@ __global__ void nb_scatter(BinGrid g, const uint32_t* __restrict__ cell_of,
 
 // One warp per cell: each index's rank is the number of smaller indices in
 // the cell, which undoes whatever order the scatter's atomics produced.
+// Cells of more than 32 particles are listed (in the scratch words the
+// counts no longer need) for nb_order_large.
 __global__ void nb_order(BinGrid g, const uint32_t* __restrict__ cell_start,
-                         uint32_t* __restrict__ sorted) {
+                         uint32_t* __restrict__ sorted, uint32_t* __restrict__ large) {
     const uint32_t cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (cell >= g.total) return;
@@ -139,15 +140,55 @@ __global__ void nb_order(BinGrid g, const uint32_t* __restrict__ cell_start,
         __syncwarp();
         if (lane < m) sorted[start + rank] = key;
     } else if (lane == 0) {
-        for (uint32_t s = start + 1; s < end; s++) {
-            const uint32_t key = sorted[s];
-            uint32_t t = s;
-            while (t > start && sorted[t - 1] > key) {
-                sorted[t] = sorted[t - 1];
-                t -= 1;
+        large[atomicAdd(&large[kLargeCount], 1u)] = cell;
+    }
+}
+
+// Bitonic sorting network on a[0, m) as the first m of 2^p places, the rest
+// read as +infinity: every comparator puts the smaller value first (the
+// first stage of each merge compares mirror images, i with i ^ (k - 1)), so
+// the padding never moves and comparators that reach it are skipped.
+// O(m log^2 m) work over the block's threads; the values are distinct.
+__device__ void block_bitonic(uint32_t* a, uint32_t m) {
+    uint64_t size = 1;  // up to 2^31: 64-bit, so the doubling below ends
+    while (size < m) size <<= 1;
+    for (uint64_t k = 2; k <= size; k <<= 1) {
+        for (uint64_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint64_t i = threadIdx.x; i < size; i += blockDim.x) {
+                const uint64_t l = j == (k >> 1) ? (i ^ (k - 1u)) : (i ^ j);
+                if (l > i && l < m) {
+                    const uint32_t x = a[i], y = a[l];
+                    if (y < x) {
+                        a[i] = y;
+                        a[l] = x;
+                    }
+                }
             }
-            sorted[t] = key;
+            __syncthreads();
         }
+    }
+}
+
+// The listed cells of more than 32 particles, one block each at a time:
+// sorted in shared memory up to kSharedSort particles, in place in global
+// memory beyond that.
+__global__ void __launch_bounds__(kSortThreads) nb_order_large(const uint32_t* __restrict__ cell_start,
+                                                               uint32_t* __restrict__ sorted,
+                                                               const uint32_t* __restrict__ large) {
+    __shared__ uint32_t s_keys[kSharedSort];
+    const uint32_t listed = large[kLargeCount];
+    for (uint32_t t = blockIdx.x; t < listed; t += gridDim.x) {
+        const uint32_t cell = large[t];
+        const uint32_t start = cell_start[cell], m = cell_start[cell + 1] - start;
+        if (m <= kSharedSort) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s_keys[i] = sorted[start + i];
+            __syncthreads();
+            block_bitonic(s_keys, m);
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) sorted[start + i] = s_keys[i];
+        } else {
+            block_bitonic(sorted + start, m);
+        }
+        __syncthreads();
     }
 }
 
@@ -191,7 +232,9 @@ extern "C" vlj_status vlj_bin_noalloc(const double* pos, size_t count, const dou
         vlj::nb_scan<<<1, 1024, 0, s>>>(g, counts, cell_start);
         vlj::nb_scatter<<<blocks, 256, 0, s>>>(g, cell_of, cell_start, counts, sorted);
         vlj::nb_order<<<(unsigned)(((uint64_t)g.total * 32u + 255u) / 256u), 256, 0, s>>>(
-            g, cell_start, sorted);
+            g, cell_start, sorted, counts);
+        vlj::nb_order_large<<<vlj::kLargeBlocks, vlj::kSortThreads, 0, s>>>(cell_start, sorted,
+                                                                          counts);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return fail(VLJ_CUDA_ERROR, "bin_noalloc: %s", cudaGetErrorString(e));

@@ -63,6 +63,21 @@ def fp32_peak():
     return t.value
 
 
+def philox(ctr, key):
+    """The device's noise stream for known-answer checks: Philox-4x32-10 of
+    each counter (n x 4 uint32) and key (n x 2 uint32), and the three Gaussian
+    numbers the step kernel draws for (id, step, seed) = (ctr[:, 0],
+    ctr[:, 1] + 2^32 ctr[:, 2], key[:, 0]). Returns (words n x 4, noise n x 3)."""
+    ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
+    key = np.ascontiguousarray(key, dtype=np.uint32).reshape(-1, 2)
+    if len(ctr) != len(key):
+        raise ValueError("one key per counter")
+    out = np.zeros((len(ctr), 4), np.uint32)
+    noise = np.zeros((len(ctr), 3), np.float32)
+    _check(_lib.vlj_debug_philox(ptr(ctr), ptr(key), len(ctr), ptr(out), ptr(noise)))
+    return out, noise
+
+
 def launches():
     """Kernel launches this library has made in this process."""
     n = C.c_uint64()
