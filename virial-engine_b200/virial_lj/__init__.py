@@ -74,7 +74,8 @@ def philox(ctr, key):
         raise ValueError("one key per counter")
     out = np.zeros((len(ctr), 4), np.uint32)
     noise = np.zeros((len(ctr), 3), np.float32)
-    _check(_lib.vlj_debug_philox(ptr(ctr), ptr(key), len(ctr), ptr(out), ptr(noise)))
+    _check(_lib.vlj_debug_philox(_ffi.ptr(ctr), _ffi.ptr(key), len(ctr), _ffi.ptr(out),
+                                 _ffi.ptr(noise)))
     return out, noise
 
 
