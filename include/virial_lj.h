@@ -329,6 +329,18 @@ VLJ_API vlj_status vlj_debug_kernel_time(vlj_sim *sim, double *total_ms, uint64_
 /* FP32 FMA throughput of the current device in TFLOP/s (a calibration kernel
  * of independent FMA chains on every SM). */
 VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
+/* Cell tiles of the step kernel (single boxes of four or more particles per
+ * cell on average): 0 switches the step kernel back to per-particle gathers
+ * from the slot list (same trajectory to the bit); tile_info gives the
+ * bricks per x-row, the bricks in all, the tile capacity (particles a block
+ * stages) and the threads per block (all 0 without tiles). read_tile_lists
+ * copies the 16-bit tile lists (capacity rounded up to 8 rows of `segment`
+ * x 8 entries: entry k of sorted position p at [(k / 8) * segment * 8 + p * 8
+ * + k % 8]) after bringing the lists up to date. */
+VLJ_API vlj_status vlj_debug_set_tiles(vlj_sim *sim, int on);
+VLJ_API vlj_status vlj_debug_tile_info(vlj_sim *sim, uint32_t *brick_cols, uint32_t *bricks,
+                                       uint32_t *tile_cap, uint32_t *threads);
+VLJ_API vlj_status vlj_debug_read_tile_lists(vlj_sim *sim, uint16_t *out);
 /* The Langevin noise stream as the device computes it (known-answer checks):
  * for k < n, out[4k..4k+3] = Philox-4x32-10 of counter ctr[4k..4k+3] and key
  * key[2k..2k+1], and noise[3k..3k+2] = the three Gaussian numbers the step

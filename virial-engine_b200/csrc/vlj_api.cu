@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -769,6 +770,39 @@ vlj_status vlj_debug_fp32_peak(double* tflops) {
     return VLJ_OK;
 }
 
+vlj_status vlj_debug_set_tiles(vlj_sim* s, int on) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    const bool want = on != 0;
+    if (want == s->tiles_on) return VLJ_OK;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    sim_drop_step_graphs(s);
+    s->tiles_on = want;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_tile_info(vlj_sim* s, uint32_t* brick_cols, uint32_t* bricks,
+                               uint32_t* tile_cap, uint32_t* threads) {
+    if (!s || !brick_cols || !bricks || !tile_cap || !threads)
+        return fail(VLJ_INVALID_ARG, "null argument");
+    const bool tiles = s->replicas.empty() && s->arena.list16;
+    *brick_cols = tiles ? s->box.brick_cols : 0u;
+    *bricks = tiles ? s->arena.bricks : 0u;
+    *tile_cap = tiles ? s->arena.tile_cap : 0u;
+    *threads = tiles ? s->arena.tile_threads : 0u;
+    return VLJ_OK;
+}
+
+vlj_status vlj_debug_read_tile_lists(vlj_sim* s, uint16_t* out) {
+    if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
+    if (!s->arena.list16) return fail(VLJ_NOT_ENABLED, "this simulation has no cell tiles");
+    TRY(lists_now(s));
+    const size_t rows = (s->box.capacity + 7) / 8;
+    CUDA_TRY(cudaMemcpyAsync(out, s->arena.list16, sizeof(uint16_t) * 8 * (size_t)s->arena.seg * rows,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VLJ_OK;
+}
+
 vlj_status vlj_debug_philox(const uint32_t* ctr, const uint32_t* key, size_t n, uint32_t* out,
                             float* noise) {
     if (!ctr || !key || !out || !noise) return fail(VLJ_INVALID_ARG, "null argument");
@@ -855,6 +889,50 @@ vlj_status check_fault(vlj_sim* s) {
 
 vlj_status sim_lists_now(vlj_sim* s) { return lists_now(s); }
 
+// Cell tiles for the step kernel of a single box (tile_step_kernel): bricks
+// of whole cells along x sized for about 112 home particles at the box's
+// occupancy (its mean, or 0.9 particles per unit volume if that is more: a
+// liquid region in a box that is mostly vapour), one block each; a tile
+// holds nine rows of the brick's cells and one more on each side, with 30 %
+// room for density fluctuations (bricks beyond it take the slot list). Off
+// in dilute boxes (under four particles per cell on average), where each
+// particle's few neighbours cost little to gather, and when VLJ_TILES=0.
+static bool plan_tiles(Box& b, Arena& a) {
+    b.brick_cols = 0u;
+    b.brick_base = 0u;
+    a.bricks = a.tile_cap = a.tile_threads = 0u;
+    const char* env = std::getenv("VLJ_TILES");
+    if (env && env[0] == '0') return false;
+    const double cells = (double)b.total_cells;
+    const double mean = (double)b.n / cells;
+    if (mean < 4.0) return false;
+    const double occupancy = std::max(mean, 0.9 * b.box[0] * b.box[1] * b.box[2] / cells);
+    const uint32_t nx = b.cells[0];
+    const double width = std::max(1.0, std::round(112.0 / occupancy));
+    uint32_t cols = (uint32_t)std::ceil((double)nx / width);
+    cols = std::max(1u, std::min(cols, nx));
+    // each tile row holds distinct cells: w + 2 <= nx, or one brick per row
+    while (cols > 1u && (nx + cols - 1u) / cols + 2u > nx) cols++;
+    const uint32_t wmax = (nx + cols - 1u) / cols;
+    const uint32_t rx = cols == 1u ? nx : wmax + 2u;
+    const double homes = wmax * occupancy;
+    uint32_t threads = 32u * (uint32_t)std::ceil(homes / 32.0);
+    threads = std::max(64u, std::min(threads, (uint32_t)kBlock));
+    uint32_t cap = 32u * (uint32_t)std::ceil(1.3 * 9.0 * rx * occupancy / 32.0);
+    cap = std::min(cap, 4096u);  // 64 KB of shared memory at most
+    // VLJ_TILE_CAP overrides the capacity (a tuning and testing knob: a small
+    // one sends blocks to the slot-list fallback)
+    if (const char* c = std::getenv("VLJ_TILE_CAP")) {
+        const long v = std::strtol(c, nullptr, 10);
+        if (v >= 16 && v <= 4096) cap = (uint32_t)v;
+    }
+    b.brick_cols = cols;
+    a.bricks = cols * b.cells[1] * b.cells[2];
+    a.tile_cap = cap;
+    a.tile_threads = threads;
+    return true;
+}
+
 vlj_status sim_allocate(vlj_sim* s, void* stream) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
@@ -940,6 +1018,10 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.rb_first, boxes.size() + 1));
     TRY(dalloc(s, &a.list_count, seg));
     TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((cap + 3) / 4)));
+    if (!batched && plan_tiles(s->box, a)) {
+        TRY(dalloc(s, &a.list16, (size_t)seg * 8 * ((cap + 7) / 8)));
+        boxes[0] = s->box;
+    }
     TRY(dalloc(s, &a.block_rows, ((size_t)seg + kForceThreads - 1) / kForceThreads));
     TRY(make_list_map(a, (cap + 3) / 4, &s->list_map));
     TRY(dalloc(s, &a.aos, 6 * (size_t)seg));
@@ -991,10 +1073,19 @@ static vlj_status end_capture(cudaStream_t cs, cudaError_t launched, cudaGraphNo
     return VLJ_OK;
 }
 
+// The arena as the step kernel sees it: without cell tiles while they are
+// switched off, or while the cell grid is rebuilt on every step (the tiles
+// follow the grid of the last list build, which that mode overwrites).
+static Arena step_arena(const vlj_sim* s) {
+    Arena a = s->arena;
+    if (!s->tiles_on || s->grid_every_step) a.tile_threads = 0;
+    return a;
+}
+
 // What follows the rebuild in a step: the fused step kernel, or on canonical
 // velocities the force pass (and the exchange's apply pass).
 static cudaError_t launch_step_tail(vlj_sim* s, cudaStream_t cs) {
-    if (!s->canonical()) return launch_step(s->arena, s->list_map, s->shifted_force, cs);
+    if (!s->canonical()) return launch_step(step_arena(s), s->list_map, s->shifted_force, cs);
     cudaError_t e = launch_canon_force(s->arena, s->list_map, s->shifted_force,
                                        s->nose_hoover ? kNoseHoover : kExchange, cs);
     if (e == cudaSuccess && s->exchange) e = launch_hex_apply(s->arena, cs);
@@ -1052,7 +1143,7 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out,
         CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, &n_cond, nullptr, 1, mode));
         cudaError_t e;
         if (fold)
-            e = launch_step(s->arena, s->list_map, s->shifted_force, cs,
+            e = launch_step(step_arena(s), s->list_map, s->shifted_force, cs,
                             k + 1 < count ? (unsigned long long)h[k + 1] : 0ull, heat && k == 0);
         else
             e = launch_step_tail(s, cs);
@@ -1110,11 +1201,11 @@ static vlj_status step_direct(vlj_sim* s, bool heat = false) {
             s->ev_end.push_back(b);
         }
         CUDA_TRY(cudaEventRecord(s->ev_start[s->ev_used], s->stream));
-        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream, 0, heat));
+        CUDA_TRY(launch_step(step_arena(s), s->list_map, s->shifted_force, s->stream, 0, heat));
         CUDA_TRY(cudaEventRecord(s->ev_end[s->ev_used], s->stream));
         s->ev_used++;
     } else {
-        CUDA_TRY(launch_step(s->arena, s->list_map, s->shifted_force, s->stream, 0, heat));
+        CUDA_TRY(launch_step(step_arena(s), s->list_map, s->shifted_force, s->stream, 0, heat));
     }
     return VLJ_OK;
 }

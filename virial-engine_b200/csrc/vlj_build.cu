@@ -41,7 +41,7 @@ namespace vlj {
 #define VLJ_BUILD_ROUND 128
 #endif
 #ifndef VLJ_BUILD_STAGE
-#define VLJ_BUILD_STAGE 512
+#define VLJ_BUILD_STAGE 448
 #endif
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
@@ -93,6 +93,11 @@ __device__ __forceinline__ void store_if(bool p, uint32_t* ptr, uint32_t v) {
                  ::"l"(ptr), "r"(v), "r"((uint32_t)p) : "memory");
 }
 
+__device__ __forceinline__ void store16_if(bool p, uint16_t* ptr, uint32_t v) {
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %2, 0;\n @q st.global.u16 [%0], %1;\n}"
+                 ::"l"(ptr), "h"((unsigned short)v), "r"((uint32_t)p) : "memory");
+}
+
 // Whether stencil offset d (-1, 0, 1) along an axis of n cells reaches a cell
 // an earlier offset already did: with two cells -1 and +1 are the same
 // neighbour, with one cell every offset is the home cell. Boxes of three or
@@ -108,6 +113,8 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     // staged candidates: (x, y, z) as f32 offsets from the home cell's centre
     // (wide boxes) or as encoded words (narrow ones), the slot in w
     __shared__ uint4 s_cand[kBuildWarps][kStage];
+    // with cell tiles: each staged candidate's index in the brick's tile
+    __shared__ uint16_t s_tix[kBuildWarps][kStage];
     __shared__ uint4 s_home[kBuildWarps][32];
     for (int t = threadIdx.x; t < 512; t += blockDim.x)
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
@@ -169,6 +176,35 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
         const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
         off -= cnt;  // exclusive; lanes 27..31 sit at `total`
 
+        // With cell tiles: lane s's stencil cell's first particle's index in
+        // the tile of the home cell's brick (tile_step_kernel stages the same
+        // tile), and the home cell's own (stencil lane 13).
+        const bool tiles = a.list16 != nullptr && bx.brick_cols != 0u;
+        uint32_t tbase = 0;
+        if (tiles) {
+            const Brick k = make_brick(bx, brick_col_of(bx, (uint32_t)c[0]), (uint32_t)c[1],
+                                       (uint32_t)c[2]);
+            uint32_t rowc = lane < 9u ? tile_row_prefix(a.cell_start, bx, k,
+                                                        tile_row_cell(bx, k, lane), k.rx)
+                                      : 0u;
+            uint32_t incl = rowc;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += t;
+            }
+            // lane s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1) lies in tile row s / 3
+            const uint32_t row_base = __shfl_sync(0xffffffffu, incl - rowc, min(lane / 3u, 8u));
+            if (lane < 27u) {
+                const uint32_t rho = lane / 3u;
+                tbase = row_base + tile_row_prefix(a.cell_start, bx, k, tile_row_cell(bx, k, rho),
+                                                   tile_col(bx, k, (uint32_t)c[0],
+                                                            (int32_t)(lane % 3u) - 1));
+            }
+        }
+        const uint32_t home_tix0 = __shfl_sync(0xffffffffu, tbase, 13) - cs0;
+        const uint32_t row16_stride = a.seg * 8u;  // entries between a position's rows
+
         // The home cell as an interval of encoded coordinates per axis, for the
         // staging filter: a candidate farther than reach_r2 from the whole home
         // cell cannot be in any home particle's list.
@@ -219,7 +255,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 // Fetch the next kRound candidates of the stream (kRound / 32 per
                 // lane, loads in flight together), keep those within reach of the
                 // home cell, and stage them in stream order.
-                uint32_t j[kRound / 32];
+                uint32_t j[kRound / 32], tix[kRound / 32];
 #pragma unroll
                 for (int r = 0; r < kRound / 32; r++) {
                     const uint32_t t = base + (uint32_t)r * 32u + lane;
@@ -235,6 +271,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                     const uint32_t from = __shfl_sync(0xffffffffu, cs, lo);
                     const uint32_t at = __shfl_sync(0xffffffffu, off, lo);
                     j[r] = t < total ? a.sorted[from + t - at] : 0xffffffffu;
+                    tix[r] = __shfl_sync(0xffffffffu, tbase, lo) + t - at;
                 }
                 uint4 pe[kRound / 32];
 #pragma unroll
@@ -268,6 +305,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                                 __float_as_uint((float)(int32_t)(pe[r].z - mid[2]) * dec[2]), j[r]);
                         else
                             s_cand[warp][to] = make_uint4(pe[r].x, pe[r].y, pe[r].z, j[r]);
+                        if (tiles) s_tix[warp][to] = (uint16_t)tix[r];
                     }
                     staged += (uint32_t)__popc(kept_mask);
                 }
@@ -287,6 +325,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                     const uint32_t q = c0 + lane;
                     const bool valid = q < staged;
                     const uint4 e = s_cand[warp][valid ? q : 0u];
+                    const uint32_t e_tix = tiles ? s_tix[warp][valid ? q : 0u] : 0u;
                     auto settle = [&](uint32_t h, uint32_t home_slot, float r2e) {
                         const bool near = valid && r2e < pre_r2 && e.w != home_slot;
                         bool take = near && r2e < acc_r2;
@@ -300,6 +339,13 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                                  a.list + ((unsigned long long)(k >> 2) * row_stride +
                                            (home_slot * 4u + (k & 3u))),
                                  e.w);
+                        // entry k of the 16-bit list of the home's sorted
+                        // position h0 + h: row k / 8, place k % 8
+                        if (tiles)
+                            store16_if(take && k < cap,
+                                       a.list16 + ((unsigned long long)(k >> 3) * row16_stride +
+                                                   ((h0 + h) * 8u + (k & 7u))),
+                                       e_tix);
                         if (lane == h) found += (uint32_t)__popc(m);
                     };
                     if (wide) {
@@ -330,6 +376,13 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 uint32_t* row_of_i = a.list + (size_t)i * 4u;
                 for (uint32_t k = kept; k & 3u; k++)
                     row_of_i[(size_t)(k >> 2) * row_stride + (k & 3u)] = i;
+                if (tiles) {
+                    // the home's own tile index: a zero separation, skipped
+                    uint16_t* row16 = a.list16 + (size_t)(h0 + lane) * 8u;
+                    const uint16_t own_tix = (uint16_t)(home_tix0 + h0 + lane);
+                    for (uint32_t k = kept; k & 7u; k++)
+                        row16[(size_t)(k >> 3) * row16_stride + (k & 7u)] = own_tix;
+                }
                 a.list_count[i] = kept;
                 if (found > cap) atomicMax(&a.ctrl[b].overflow, found);
                 a.snap[i] = own_enc;

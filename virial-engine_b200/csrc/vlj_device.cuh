@@ -57,6 +57,79 @@ __device__ __forceinline__ uint32_t cell_parts(uint32_t m, bool narrow) {
     return narrow ? min(kMaxParts, (m + kPartHomes - 1u) / kPartHomes) : 1u;
 }
 
+// ---- cell tiles (tile_step_kernel, and the list build that indexes them) ----
+// A brick is cells x0 .. x0 + w - 1 of the x-row (y, z) of a box. Its tile is
+// the nine x-rows (y + dy, z + dz), dz, dy = -1..1 in that order, each over
+// the rx cells x_start, x_start + 1, ... (mod nx): the whole row when the row
+// is one brick, else the brick's cells and one more on each side. Each cell
+// brings its particles in sorted order, so the tile holds every home
+// particle's neighbour cells, and the cells of one row are at most two runs
+// of the sorted order.
+struct Brick {
+    uint32_t x0, w, rx, x_start;
+    uint32_t y, z;
+    bool full;  // the row is one brick
+};
+
+// Bricks per x-row r_n = brick_cols: widths nx / r_n, the first nx % r_n one more.
+__device__ __forceinline__ void brick_span(const Box& bx, uint32_t r, uint32_t& x0, uint32_t& w) {
+    const uint32_t nx = bx.cells[0], cols = bx.brick_cols;
+    const uint32_t q = nx / cols, rem = nx % cols;
+    w = q + (r < rem ? 1u : 0u);
+    x0 = r * q + min(r, rem);
+}
+
+__device__ __forceinline__ uint32_t brick_col_of(const Box& bx, uint32_t cx) {
+    const uint32_t nx = bx.cells[0], cols = bx.brick_cols;
+    const uint32_t q = nx / cols, rem = nx % cols;
+    const uint32_t wide = rem * (q + 1u);
+    return cx < wide ? cx / (q + 1u) : rem + (cx - wide) / q;
+}
+
+__device__ __forceinline__ Brick make_brick(const Box& bx, uint32_t r, uint32_t y, uint32_t z) {
+    Brick k;
+    brick_span(bx, r, k.x0, k.w);
+    k.y = y;
+    k.z = z;
+    k.full = bx.brick_cols == 1u;
+    const uint32_t nx = bx.cells[0];
+    k.rx = k.full ? nx : k.w + 2u;
+    k.x_start = k.full ? 0u : (k.x0 + nx - 1u) % nx;
+    return k;
+}
+
+// Brick `index` of a box: (z * ny + y) * brick_cols + r.
+__device__ __forceinline__ Brick brick_at(const Box& bx, uint32_t index) {
+    const uint32_t cols = bx.brick_cols;
+    const uint32_t r = index % cols, yz = index / cols;
+    return make_brick(bx, r, yz % bx.cells[1], yz / bx.cells[1]);
+}
+
+// First cell of tile row rho (0..8: dz = rho / 3 - 1, dy = rho % 3 - 1).
+__device__ __forceinline__ uint32_t tile_row_cell(const Box& bx, const Brick& k, uint32_t rho) {
+    const uint32_t ny = bx.cells[1], nz = bx.cells[2];
+    const uint32_t y = (k.y + ny + (rho % 3u) - 1u) % ny;
+    const uint32_t z = (k.z + nz + (rho / 3u) - 1u) % nz;
+    return bx.cell_base + (z * ny + y) * bx.cells[0];
+}
+
+// Particles in the first xp cells of a tile row whose cells start at `row`
+// (xp <= rx): one run of the sorted order, or two where the row wraps.
+__device__ __forceinline__ uint32_t tile_row_prefix(const uint32_t* __restrict__ cs,
+                                                    const Box& bx, const Brick& k, uint32_t row,
+                                                    uint32_t xp) {
+    const uint32_t nx = bx.cells[0];
+    const uint32_t end = k.x_start + xp;
+    if (end <= nx) return cs[row + end] - cs[row + k.x_start];
+    return cs[row + nx] - cs[row + k.x_start] + cs[row + end - nx] - cs[row];
+}
+
+// Tile column of home cell cx's neighbour at dx (-1, 0, 1).
+__device__ __forceinline__ uint32_t tile_col(const Box& bx, const Brick& k, uint32_t cx, int32_t dx) {
+    const uint32_t nx = bx.cells[0];
+    return k.full ? (cx + nx + (uint32_t)dx) % nx : cx - k.x0 + 1u + (uint32_t)dx;
+}
+
 // Whether the cell grid is rebuilt this step: with the lists, or on every
 // step when grid_every_step is set (a single box).
 __device__ __forceinline__ bool grid_pass(const Arena& a) {

@@ -113,12 +113,59 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
 }
 
 // ---- forces from the list (lennard_jones.wgsl:503-545) ----
-// Separations come from the 32-bit box fractions: the wrapped integer
-// difference is the nearest image. The force factor is the same expression
-// in every pass, so the step, the first forces and the measurement agree to
-// the bit. With ENERGIES the particle's halves of pair energy and virial are
-// also summed, as unevaluated f32 pairs (as the reference sums them in
-// double-float, lennard_jones.wgsl:518-519). Every thread of the block must
+// One list entry's terms into the particle's sums: the separation from the
+// 32-bit box fractions (the wrapped integer difference is the nearest
+// image), the force factor (the same expression in every pass, so the step,
+// the first forces and the measurement agree to the bit), and with ENERGIES
+// the halves of the pair energy and virial as unevaluated f32 pairs (as the
+// reference sums them in double-float, lennard_jones.wgsl:518-519). A zero
+// separation (the padding of a list's last row) adds nothing.
+template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT>
+__device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const uint4 pj,
+                                           const Box& bx, float dec0, float dec1, float dec2,
+                                           uint32_t rc2_bits_m1, float fshift) {
+    const float dx = decode_diff(pj.x, own.x, dec0);
+    const float dy = decode_diff(pj.y, own.y, dec1);
+    const float dz = decode_diff(pj.z, own.z, dec2);
+    const float r2 = sep_r2(dx, dy, dz);
+    const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
+    // branch-free: most list entries are inside the cutoff; the select
+    // drops whatever the pair math gives for entries that are not
+    const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
+    s.ax = __fmaf_rn(-dx, f, s.ax);
+    s.ay = __fmaf_rn(-dy, f, s.ay);
+    s.az = __fmaf_rn(-dz, f, s.az);
+    if (HEAT) {
+        s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
+        const float fx = dx * f, fy = dy * f, fz = dz * f;
+        s.t[0] += dx * fx;
+        s.t[1] += dy * fy;
+        s.t[2] += dz * fz;
+        s.t[3] += dx * fy;
+        s.t[4] += dx * fz;
+        s.t[5] += dy * fz;
+    }
+    if (ENERGIES && in) {
+        // The sums take r^2 rounded once from the exact separation (the
+        // integer differences times the box step are exact in f64): on a
+        // lattice, where every pair at one distance rounds alike, the f32
+        // components' three roundings would bias the virial coherently.
+        const double ex = (double)(int32_t)(pj.x - own.x) * (double)dec0;
+        const double ey = (double)(int32_t)(pj.y - own.y) * (double)dec1;
+        const double ez = (double)(int32_t)(pj.z - own.z) * (double)dec2;
+        float rf, u, t, e;
+        lj_pair<SHIFTED_FORCE>((float)(ex * ex + ey * ey + ez * ez), bx, rf, u);
+        two_sum(s.pe, 0.5f * u, t, e);
+        s.pe = t;
+        s.pe_lo += e;
+        two_sum(s.w, 0.5f * rf, t, e);
+        s.w = t;
+        s.w_lo += e;
+        s.near += r2 < 2.25f ? 1u : 0u;
+    }
+}
+
+// The particle's pair sums over its list. Every thread of the block must
 // call this: it synchronises the block between tiles.
 template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT = false>
 __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap* map,
@@ -155,47 +202,10 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     // 0 < r2 < rc2 as one unsigned comparison of the bit patterns (r2 >= +0)
     const uint32_t rc2_bits_m1 = __float_as_uint(rc2) - 1u;
     // The list's last row is padded with the particle itself, whose zero
-    // separation drops out here with the entries beyond the cutoff.
+    // separation drops out with the entries beyond the cutoff.
     auto accumulate = [&](const uint4 pj) {
-        const float dx = decode_diff(pj.x, own.x, dec0);
-        const float dy = decode_diff(pj.y, own.y, dec1);
-        const float dz = decode_diff(pj.z, own.z, dec2);
-        const float r2 = sep_r2(dx, dy, dz);
-        const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
-        // branch-free: most list entries are inside the cutoff; the select
-        // drops whatever the pair math gives for entries that are not
-        const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
-        s.ax = __fmaf_rn(-dx, f, s.ax);
-        s.ay = __fmaf_rn(-dy, f, s.ay);
-        s.az = __fmaf_rn(-dz, f, s.az);
-        if (HEAT) {
-            s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
-            const float fx = dx * f, fy = dy * f, fz = dz * f;
-            s.t[0] += dx * fx;
-            s.t[1] += dy * fy;
-            s.t[2] += dz * fz;
-            s.t[3] += dx * fy;
-            s.t[4] += dx * fz;
-            s.t[5] += dy * fz;
-        }
-        if (ENERGIES && in) {
-            // The sums take r^2 rounded once from the exact separation (the
-            // integer differences times the box step are exact in f64): on a
-            // lattice, where every pair at one distance rounds alike, the f32
-            // components' three roundings would bias the virial coherently.
-            const double ex = (double)(int32_t)(pj.x - own.x) * (double)dec0;
-            const double ey = (double)(int32_t)(pj.y - own.y) * (double)dec1;
-            const double ez = (double)(int32_t)(pj.z - own.z) * (double)dec2;
-            float rf, u, t, e;
-            lj_pair<SHIFTED_FORCE>((float)(ex * ex + ey * ey + ez * ez), bx, rf, u);
-            two_sum(s.pe, 0.5f * u, t, e);
-            s.pe = t;
-            s.pe_lo += e;
-            two_sum(s.w, 0.5f * rf, t, e);
-            s.w = t;
-            s.w_lo += e;
-            s.near += r2 < 2.25f ? 1u : 0u;
-        }
+        pair_terms<SHIFTED_FORCE, ENERGIES, HEAT>(s, own, pj, bx, dec0, dec1, dec2, rc2_bits_m1,
+                                                  fshift);
     };
 
 #if VLJ_LIST_STREAM
@@ -295,7 +305,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
 // series slot 1 + 3 * sample: one atomic each (integer sums, any order).
 __device__ __forceinline__ void block_sum_series(const Arena& a, const long long (&raw)[3],
                                                  uint32_t sample) {
-    __shared__ long long s_sum[kForceThreads / 32][3];
+    __shared__ long long s_sum[kBlock / 32][3];  // blocks of up to kBlock threads
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -307,7 +317,7 @@ __device__ __forceinline__ void block_sum_series(const Arena& a, const long long
     __syncthreads();
     if (threadIdx.x < 3) {
         long long x = 0;
-        for (int w = 0; w < kForceThreads / 32; w++) x += s_sum[w][threadIdx.x];
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) x += s_sum[w][threadIdx.x];
         if (x) atomicAdd(&a.series[1 + 3 * (size_t)sample + threadIdx.x], (unsigned long long)x);
     }
 }
@@ -334,6 +344,64 @@ __device__ __forceinline__ void langevin_noise(uint32_t id, unsigned long long s
     xi[0] = ra * cosf(aa);
     xi[1] = ra * sinf(aa);
     xi[2] = rb * cosf(ab);
+}
+
+// The heat current of slot i in the state a step starts from, as the
+// sampling kernel takes it: J_i = e_i v_i + T_i v_i / 2 with the canonical
+// velocity v_i = v + a dt / 2 (one box, velocities half a kick behind), each
+// component to 32.32 fixed point, added into raw.
+__device__ __forceinline__ void heat_terms(const Arena& a, const Box& bx, uint32_t i,
+                                           const PairSums& s, long long (&raw)[3]) {
+    const float acc3[3] = {s.ax, s.ay, s.az};
+    double v[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) v[c] = canonical_velocity(a, bx, 0, i, c, acc3[c]);
+    const double e = 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + (double)s.e_half;
+    const double tv[3] = {s.t[0] * v[0] + s.t[3] * v[1] + s.t[4] * v[2],
+                          s.t[3] * v[0] + s.t[1] * v[1] + s.t[5] * v[2],
+                          s.t[4] * v[0] + s.t[5] * v[1] + s.t[2] * v[2]};
+#pragma unroll
+    for (int c = 0; c < 3; c++) raw[c] += fixed_raw_f64(e * v[c] + 0.5 * tv[c]);
+}
+
+// begin + force_kick of the reference for slot i (lennard_jones.wgsl:204-276,
+// 556-574), with its forces in s: the stored velocity is half a kick behind,
+// so the two half kicks go on together, then the drift: x += v dt (constant
+// energy), or the Langevin A-O-A: x += v dt/2; v = c1 v + c2 xi; x += v dt/2.
+// State in f64; the new position goes to the other cache copy (neighbours
+// still read this step's). Returns the squared displacement since the last
+// list build.
+__device__ __forceinline__ float advance_slot(const Arena& a, const Box& bx, uint32_t i,
+                                              uint32_t phase, const PairSums& s) {
+    const float acc[3] = {s.ax, s.ay, s.az};
+    float xi[3] = {0.0f, 0.0f, 0.0f};
+    const bool langevin = bx.thermostat == 1;
+    if (langevin) langevin_noise(a.id[i], a.glob->step, bx.seed, xi);
+    const uint4 snap = a.snap[i];
+    const uint32_t sw[3] = {snap.x, snap.y, snap.z};
+    uint32_t enc[3];
+    float disp2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const size_t q = (size_t)k * a.seg + i;
+        double x = a.x[q];
+        double v = a.v[q] + (double)acc[k] * bx.dt;
+        if (langevin) {
+            x += v * bx.half_dt;
+            v = bx.c1 * v + bx.c2 * (double)xi[k];
+            x += v * bx.half_dt;
+        } else {
+            x += v * bx.dt;
+        }
+        x = wrap(x, bx.box[k]);
+        a.x[q] = x;
+        a.v[q] = v;
+        enc[k] = encode(x, bx.enc[k]);
+        const float d = decode_diff(enc[k], sw[k], bx.dec[k]);
+        disp2 += d * d;
+    }
+    a.cache[phase ^ 1u][i] = make_uint4(enc[0], enc[1], enc[2], 0u);
+    return disp2;
 }
 
 // ---- prime (lennard_jones.wgsl:547-553): first forces; the stored velocity
@@ -377,58 +445,146 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     const PairSums s =
         block_pair_sums<SHIFTED_FORCE, false, HEAT>(st, &map, a, bx, i, valid, a.cache[phase]);
     if (HEAT) {
-        // the heat current of the state this step starts from, as the
-        // sampling kernel would take it: J_i = e_i v_i + T_i v_i / 2 with the
-        // canonical velocity v_i = v + a dt / 2 (one box, velocities half a
-        // kick behind)
         const uint32_t sample = a.glob->heat_next;
         long long raw[3] = {0, 0, 0};
-        if (valid) {
-            const float acc3[3] = {s.ax, s.ay, s.az};
-            double v[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) v[c] = canonical_velocity(a, bx, 0, i, c, acc3[c]);
-            const double e = 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + (double)s.e_half;
-            const double tv[3] = {s.t[0] * v[0] + s.t[3] * v[1] + s.t[4] * v[2],
-                                  s.t[3] * v[0] + s.t[1] * v[1] + s.t[5] * v[2],
-                                  s.t[4] * v[0] + s.t[5] * v[1] + s.t[2] * v[2]};
-#pragma unroll
-            for (int c = 0; c < 3; c++) raw[c] = fixed_raw_f64(e * v[c] + 0.5 * tv[c]);
-        }
+        if (valid) heat_terms(a, bx, i, s, raw);
         block_sum_series(a, raw, sample);
     }
     float disp2 = 0.0f;
-    if (valid) {
-        const float acc[3] = {s.ax, s.ay, s.az};
-        float xi[3] = {0.0f, 0.0f, 0.0f};
-        const bool langevin = bx.thermostat == 1;
-        if (langevin) langevin_noise(a.id[i], a.glob->step, bx.seed, xi);
-        const uint4 snap = a.snap[i];
-        const uint32_t sw[3] = {snap.x, snap.y, snap.z};
-        uint32_t enc[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const size_t q = (size_t)k * a.seg + i;
-            double x = a.x[q];
-            double v = a.v[q] + (double)acc[k] * bx.dt;
-            if (langevin) {
-                x += v * bx.half_dt;
-                v = bx.c1 * v + bx.c2 * (double)xi[k];
-                x += v * bx.half_dt;
-            } else {
-                x += v * bx.dt;
-            }
-            x = wrap(x, bx.box[k]);
-            a.x[q] = x;
-            a.v[q] = v;
-            enc[k] = encode(x, bx.enc[k]);
-            const float d = decode_diff(enc[k], sw[k], bx.dec[k]);
-            disp2 += d * d;
-        }
-        a.cache[phase ^ 1u][i] = make_uint4(enc[0], enc[1], enc[2], 0u);
-    }
+    if (valid) disp2 = advance_slot(a, bx, i, phase, s);
     block_max_per_box(a, valid, b, blockIdx.x * kForceThreads, disp2);
     if (i == 0) a.glob->pending = 1u;
+    if (!next && !HEAT) return;
+    // the last block to finish takes the next step's rebuild decision and
+    // moves the heat-current series on
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&a.glob->blocks_done, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        a.glob->blocks_done = 0u;
+        if (HEAT) a.glob->heat_next += 1u;
+    }
+    if (next) decide_block(a, next, true);
+}
+
+// ---- one step over cell tiles: the same step as step_kernel, with the
+// neighbour positions staged in shared memory ----
+// A block takes one brick (a run of cells along x in one row of the box; the
+// bricks tile the box) and stages its tile -- the encoded positions of every
+// particle in the nine neighbour rows of those cells, each row one or two
+// runs of the sorted order -- in shared memory, 16 B a particle. Its threads
+// take the brick's home particles in sorted order; each walks its list as
+// 16-bit tile indices (eight to a 16-byte row, streamed past L1), so every
+// neighbour read is a shared-memory load instead of a scattered global
+// gather. The list order and the pair arithmetic are step_kernel's, so the
+// step is the same to the bit. A brick whose tile would not fit in
+// a.tile_cap entries walks the slot list with global gathers instead.
+template <bool SHIFTED_FORCE, bool HEAT>
+__global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphConditionalHandle next) {
+    count_kernel(a);
+    extern __shared__ __align__(16) uint4 s_tile[];
+    __shared__ uint32_t s_run[9][3];  // per tile row: first run's sorted start, its length, second run's start
+    __shared__ uint32_t s_base[10];   // tile index of each row's first particle; [9]: the tile's size
+    __shared__ uint32_t s_home[3];    // the brick's home particles' sorted range; [2]: first one's tile index
+    const uint32_t phase = a.glob->phase;
+    const uint4* __restrict__ cur = a.cache[phase];
+    const Box& bx = a.boxes[0];
+    const Brick k = brick_at(bx, blockIdx.x - bx.brick_base);
+    const uint32_t* __restrict__ cs = a.cell_start;
+    if (threadIdx.x < 9u) {
+        const uint32_t row = tile_row_cell(bx, k, threadIdx.x);
+        const uint32_t nx = bx.cells[0], end = k.x_start + k.rx;
+        const uint32_t first = cs[row + k.x_start];
+        const uint32_t len1 = cs[row + min(end, nx)] - first;
+        const uint32_t len2 = end > nx ? cs[row + end - nx] - cs[row] : 0u;
+        s_run[threadIdx.x][0] = first;
+        s_run[threadIdx.x][1] = len1;
+        s_run[threadIdx.x][2] = cs[row];
+        s_base[threadIdx.x + 1] = len1 + len2;
+    } else if (threadIdx.x == 32u) {
+        const uint32_t row = tile_row_cell(bx, k, 4u);
+        s_home[0] = cs[row + k.x0];
+        s_home[1] = cs[row + k.x0 + k.w];
+        s_home[2] = tile_row_prefix(cs, bx, k, row, tile_col(bx, k, k.x0, 0));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_base[0] = 0u;
+        for (int r = 0; r < 9; r++) s_base[r + 1] += s_base[r];
+    }
+    __syncthreads();
+    const uint32_t tile_size = s_base[9];
+    const bool staged = tile_size <= a.tile_cap;
+    if (staged) {
+        for (uint32_t t = threadIdx.x; t < tile_size; t += blockDim.x) {
+            uint32_t rho = 0;
+            while (t >= s_base[rho + 1]) rho++;
+            const uint32_t q = t - s_base[rho];
+            const uint32_t p = q < s_run[rho][1] ? s_run[rho][0] + q : s_run[rho][2] + (q - s_run[rho][1]);
+            s_tile[t] = cur[a.sorted[p]];
+        }
+    }
+    __syncthreads();
+    const uint32_t h0 = s_home[0], h1 = s_home[1];
+    const uint32_t own0 = s_base[4] + s_home[2] - h0;  // tile index of home p: own0 + p
+    const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2];
+    const float fshift = bx.force_shift;
+    const uint32_t rc2_bits_m1 = __float_as_uint(bx.rc2) - 1u;
+    float disp2 = 0.0f;
+    long long raw[3] = {0, 0, 0};
+    const uint32_t sample = HEAT ? a.glob->heat_next : 0u;
+    for (uint32_t p = h0 + threadIdx.x; p < h1; p += blockDim.x) {
+        const uint32_t i = a.sorted[p];
+        const uint32_t cnt = a.list_count[i];
+        PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u,
+                      0.0f, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}};
+        if (staged) {
+            const uint4 own = s_tile[own0 + p];
+            auto add = [&](uint32_t t) {
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, s_tile[t], bx, dec0, dec1, dec2,
+                                                       rc2_bits_m1, fshift);
+            };
+            const uint4* rowp = reinterpret_cast<const uint4*>(a.list16) + p;
+            const uint32_t rows = (cnt + 7u) / 8u;
+            uint4 nxt = rows ? load_row_streaming(rowp) : make_uint4(0u, 0u, 0u, 0u);
+            for (uint32_t row = 0; row < rows; row++) {
+                const uint4 e = nxt;
+                if (row + 1u < rows) nxt = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
+                add(e.x & 0xffffu);
+                add(e.x >> 16);
+                add(e.y & 0xffffu);
+                add(e.y >> 16);
+                add(e.z & 0xffffu);
+                add(e.z >> 16);
+                add(e.w & 0xffffu);
+                add(e.w >> 16);
+            }
+        } else {
+            const uint4 own = cur[i];
+            const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;
+            const uint32_t rows = (cnt + 3u) / 4u;
+            for (uint32_t row = 0; row < rows; row++) {
+                const uint4 e = load_row_streaming(rowp + (size_t)row * a.seg);
+                const uint4 p0 = __ldg(cur + e.x), p1 = __ldg(cur + e.y);
+                const uint4 p2 = __ldg(cur + e.z), p3 = __ldg(cur + e.w);
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p0, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p1, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p2, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p3, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+            }
+        }
+        if (HEAT) heat_terms(a, bx, i, s, raw);
+        disp2 = fmaxf(disp2, advance_slot(a, bx, i, phase, s));
+    }
+    if (HEAT) block_sum_series(a, raw, sample);
+    block_max_per_box(a, true, 0u, 0u, disp2);
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.glob->pending = 1u;
     if (!next && !HEAT) return;
     // the last block to finish takes the next step's rebuild decision and
     // moves the heat-current series on
@@ -828,10 +984,33 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_fo
     return after_launch();
 }
 
+template <bool SF, bool HEAT>
+static cudaError_t launch_tile_step(const Arena& a, cudaStream_t s, cudaGraphConditionalHandle next) {
+    const size_t smem = (size_t)a.tile_cap * sizeof(uint4);
+    static size_t allowed = 0;  // dynamic shared memory the kernel was opened up to
+    if (smem > allowed) {
+        cudaError_t e = cudaFuncSetAttribute(tile_step_kernel<SF, HEAT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        cudaFuncSetAttribute(tile_step_kernel<SF, HEAT>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        allowed = smem;
+    }
+    tile_step_kernel<SF, HEAT><<<a.bricks, a.tile_threads, smem, s>>>(a, next);
+    return after_launch();
+}
+
 cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_force,
                         cudaStream_t s, unsigned long long next_decision, bool heat) {
     prefer_l1_once();
     const cudaGraphConditionalHandle next = (cudaGraphConditionalHandle)next_decision;
+    if (a.list16 && a.tile_threads) {
+        if (shifted_force)
+            return heat ? launch_tile_step<true, true>(a, s, next)
+                        : launch_tile_step<true, false>(a, s, next);
+        return heat ? launch_tile_step<false, true>(a, s, next)
+                    : launch_tile_step<false, false>(a, s, next);
+    }
     const unsigned blocks = particle_blocks(a);
     if (shifted_force) {
         if (heat) step_kernel<true, true><<<blocks, kForceThreads, 0, s>>>(a, map, next);

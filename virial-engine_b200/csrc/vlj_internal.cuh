@@ -115,7 +115,13 @@ struct Box {
     uint32_t reorder_every;
     uint32_t profile_bins;
     uint32_t canonical;  // velocities stored canonical (Nose-Hoover, heat exchange)
-    uint32_t pad;
+    // Cell tiles of the step kernel (0 bricks: off for this box). A brick is
+    // a run of cells along x in one row (y, z): each x-row holds brick_cols
+    // bricks of nx / brick_cols cells (the first nx % brick_cols one more);
+    // brick_base is the first brick of this box in the arena's numbering.
+    uint32_t brick_cols;
+    uint32_t brick_base;
+    uint32_t pad[3];
 };
 
 // Mutable per-box words.
@@ -220,6 +226,15 @@ struct Arena {
     uint32_t* rb_first;
     uint32_t* list_count;
     uint32_t* list;
+    // The same lists as 16-bit indices into the cell tile of the home
+    // particle's brick (tile_step_kernel), by sorted position: entry k of the
+    // particle at sorted position p at list16[((k / 8) * seg + p) * 8 + k % 8]
+    // (a row of eight entries is 16 B); the last row's unused places hold the
+    // particle's own tile index. Null when no box uses cell tiles.
+    uint16_t* list16;
+    uint32_t bricks;     // bricks in all boxes: the tile step kernel's grid
+    uint32_t tile_cap;   // tile entries (16 B each) a block stages in shared memory
+    uint32_t tile_threads;  // threads of a tile step block
     // per force block (kForceThreads slots), for the TMA tile ring only: rows
     // (four entries each) of the longest list in it, so a block stages only
     // the rows its particles use. Reset at each rebuild of

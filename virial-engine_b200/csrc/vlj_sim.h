@@ -42,6 +42,7 @@ struct vlj_sim {
     vlj_heat_exchange exchange_settings{};
     bool canonical() const { return nose_hoover || exchange; }
     bool grid_every_step = false;  // bin, scan, scatter, sort every step; lists on the trigger
+    bool tiles_on = true;  // the step kernel stages cell tiles (when the box has them)
     vlj::Box box{};
     // batched: one Box per replica, in slot order (empty for a single box)
     std::vector<vlj::Box> replicas;

@@ -466,6 +466,25 @@ class LennardJones:
     def set_graphs(self, on):
         _check(_lib.vlj_debug_set_graphs(self._h, int(bool(on))))
 
+    def set_tiles(self, on):
+        """Cell tiles in the step kernel on or off (same trajectory either way)."""
+        _check(_lib.vlj_debug_set_tiles(self._h, int(bool(on))))
+
+    def tile_info(self):
+        """(bricks per x-row, bricks, tile capacity, threads per block); zeros without tiles."""
+        v = [C.c_uint32() for _ in range(4)]
+        _check(_lib.vlj_debug_tile_info(self._h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def read_tile_lists(self):
+        """The 16-bit tile lists by sorted position: (n, capacity rounded up to 8)."""
+        g = self.grid_info()
+        rows = (g.capacity + 7) // 8
+        raw = np.zeros(rows * g.segment * 8, np.uint16)
+        _check(_lib.vlj_debug_read_tile_lists(self._h, _ffi.ptr(raw)))
+        return raw.reshape(rows, g.segment, 8)[:, :self._n, :].transpose(1, 0, 2).reshape(
+            self._n, rows * 8)
+
     def kernel_timing(self, on):
         _check(_lib.vlj_debug_kernel_timing(self._h, int(bool(on))))
 
