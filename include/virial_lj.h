@@ -334,9 +334,10 @@ VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
  * from the slot list (same trajectory to the bit); tile_info gives the
  * bricks per x-row, the bricks in all, the tile capacity (particles a block
  * stages) and the threads per block (all 0 without tiles). read_tile_lists
- * copies the 16-bit tile lists (capacity rounded up to 8 rows of `segment`
- * x 8 entries: entry k of sorted position p at [(k / 8) * segment * 8 + p * 8
- * + k % 8]) after bringing the lists up to date. */
+ * copies the 16-bit tile lists of the last rebuild, as vlj_debug_read_grid
+ * reads the slot lists (capacity rounded up to 8 rows of `segment` x 8
+ * entries: entry k of sorted position p at [(k / 8) * segment * 8 + p * 8 +
+ * k % 8]). */
 VLJ_API vlj_status vlj_debug_set_tiles(vlj_sim *sim, int on);
 VLJ_API vlj_status vlj_debug_tile_info(vlj_sim *sim, uint32_t *brick_cols, uint32_t *bricks,
                                        uint32_t *tile_cap, uint32_t *threads);

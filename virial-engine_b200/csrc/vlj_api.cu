@@ -795,7 +795,6 @@ vlj_status vlj_debug_tile_info(vlj_sim* s, uint32_t* brick_cols, uint32_t* brick
 vlj_status vlj_debug_read_tile_lists(vlj_sim* s, uint16_t* out) {
     if (!s || !out) return fail(VLJ_INVALID_ARG, "null argument");
     if (!s->arena.list16) return fail(VLJ_NOT_ENABLED, "this simulation has no cell tiles");
-    TRY(lists_now(s));
     const size_t rows = (s->box.capacity + 7) / 8;
     CUDA_TRY(cudaMemcpyAsync(out, s->arena.list16, sizeof(uint16_t) * 8 * (size_t)s->arena.seg * rows,
                              cudaMemcpyDeviceToHost, s->stream));
