@@ -29,6 +29,8 @@ def main():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-graphs", action="store_true",
                     help="enqueue steps as direct launches (profilers see each kernel)")
+    ap.add_argument("--no-tiles", action="store_true",
+                    help="step kernel with per-particle gathers instead of cell tiles")
     ap.add_argument("--record", default=None, metavar="DIR",
                     help="write measurements.csv (a row every --every steps), positions.npy "
                          "and run.json into DIR, in the reference's formats")
@@ -40,6 +42,8 @@ def main():
                                          shifted_force=not args.truncated))
     if args.no_graphs:
         sim.set_graphs(False)
+    if args.no_tiles:
+        sim.set_tiles(False)
     m = sim.measure_now()
     print(f"{len(p)} particles, box {box:.4f}: E {m.energy():.6f} P {m.pressure():.6f}")
     t0 = time.perf_counter()
