@@ -909,6 +909,11 @@ static bool plan_tiles(Box& b, Arena& a) {
     const uint32_t nx = b.cells[0];
     const double width = std::max(1.0, std::round(112.0 / occupancy));
     uint32_t cols = (uint32_t)std::ceil((double)nx / width);
+    // VLJ_TILE_COLS sets the bricks per x-row (a tuning knob)
+    if (const char* c = std::getenv("VLJ_TILE_COLS")) {
+        const long v = std::strtol(c, nullptr, 10);
+        if (v >= 1 && v <= (long)nx) cols = (uint32_t)v;
+    }
     cols = std::max(1u, std::min(cols, nx));
     // each tile row holds distinct cells: w + 2 <= nx, or one brick per row
     while (cols > 1u && (nx + cols - 1u) / cols + 2u > nx) cols++;

@@ -165,6 +165,32 @@ __device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const u
     }
 }
 
+// pair_terms on positions given as f32 offsets from a common origin near
+// both (the cell tiles' f32 form): the separation is their plain difference.
+template <bool SHIFTED_FORCE, bool HEAT>
+__device__ __forceinline__ void pair_terms_rel(PairSums& s, const float4 own, const float4 pj,
+                                               const Box& bx, uint32_t rc2_bits_m1, float fshift) {
+    const float dx = __fsub_rn(pj.x, own.x);
+    const float dy = __fsub_rn(pj.y, own.y);
+    const float dz = __fsub_rn(pj.z, own.z);
+    const float r2 = sep_r2(dx, dy, dz);
+    const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
+    const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
+    s.ax = __fmaf_rn(-dx, f, s.ax);
+    s.ay = __fmaf_rn(-dy, f, s.ay);
+    s.az = __fmaf_rn(-dz, f, s.az);
+    if (HEAT) {
+        s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
+        const float fx = dx * f, fy = dy * f, fz = dz * f;
+        s.t[0] += dx * fx;
+        s.t[1] += dy * fy;
+        s.t[2] += dz * fz;
+        s.t[3] += dx * fy;
+        s.t[4] += dx * fz;
+        s.t[5] += dy * fz;
+    }
+}
+
 // The particle's pair sums over its list. Every thread of the block must
 // call this: it synchronises the block between tiles.
 template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT = false>
@@ -521,13 +547,27 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
     __syncthreads();
     const uint32_t tile_size = s_base[9];
     const bool staged = tile_size <= a.tile_cap;
+#if VLJ_TILE_F32
+    // the tile as f32 offsets from the brick's centre (encoded)
+    const uint32_t org[3] = {
+        encode(((double)k.x0 + 0.5 * (double)k.w) * (double)bx.cell_size_f[0], bx.enc[0]),
+        encode(((double)k.y + 0.5) * (double)bx.cell_size_f[1], bx.enc[1]),
+        encode(((double)k.z + 0.5) * (double)bx.cell_size_f[2], bx.enc[2])};
+    float4* s_tilef = reinterpret_cast<float4*>(s_tile);
+#endif
     if (staged) {
         for (uint32_t t = threadIdx.x; t < tile_size; t += blockDim.x) {
             uint32_t rho = 0;
             while (t >= s_base[rho + 1]) rho++;
             const uint32_t q = t - s_base[rho];
             const uint32_t p = q < s_run[rho][1] ? s_run[rho][0] + q : s_run[rho][2] + (q - s_run[rho][1]);
+#if VLJ_TILE_F32
+            const uint4 w = cur[a.sorted[p]];
+            s_tilef[t] = make_float4(decode_diff(w.x, org[0], bx.dec[0]), decode_diff(w.y, org[1], bx.dec[1]),
+                                     decode_diff(w.z, org[2], bx.dec[2]), 0.0f);
+#else
             s_tile[t] = cur[a.sorted[p]];
+#endif
         }
     }
     __syncthreads();
@@ -545,26 +585,66 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
         PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u,
                       0.0f, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}};
         if (staged) {
+#if VLJ_TILE_F32
+            const float4 own = s_tilef[own0 + p];
+            auto add = [&](const float4 pj) {
+                pair_terms_rel<SHIFTED_FORCE, HEAT>(s, own, pj, bx, rc2_bits_m1, fshift);
+            };
+            auto fetch = [&](uint32_t t) { return s_tilef[t]; };
+            using Pos = float4;
+#else
             const uint4 own = s_tile[own0 + p];
-            auto add = [&](uint32_t t) {
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, s_tile[t], bx, dec0, dec1, dec2,
+            auto add = [&](const uint4 pj) {
+                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, pj, bx, dec0, dec1, dec2,
                                                        rc2_bits_m1, fshift);
             };
+            auto fetch = [&](uint32_t t) { return s_tile[t]; };
+            using Pos = uint4;
+#endif
             const uint4* rowp = reinterpret_cast<const uint4*>(a.list16) + p;
             const uint32_t rows = (cnt + 7u) / 8u;
             uint4 nxt = rows ? load_row_streaming(rowp) : make_uint4(0u, 0u, 0u, 0u);
+#if VLJ_TILE_PIPE
+            // the next row's eight neighbours are read while this row's pairs
+            // are computed
+            Pos q[8];
+            if (rows) {
+                const uint4 e = nxt;
+                if (rows > 1u) nxt = load_row_streaming(rowp + a.seg);
+                q[0] = fetch(e.x & 0xffffu); q[1] = fetch(e.x >> 16);
+                q[2] = fetch(e.y & 0xffffu); q[3] = fetch(e.y >> 16);
+                q[4] = fetch(e.z & 0xffffu); q[5] = fetch(e.z >> 16);
+                q[6] = fetch(e.w & 0xffffu); q[7] = fetch(e.w >> 16);
+            }
+            for (uint32_t row = 0; row < rows; row++) {
+                Pos c[8];
+#pragma unroll
+                for (int m = 0; m < 8; m++) c[m] = q[m];
+                if (row + 1u < rows) {
+                    const uint4 e = nxt;
+                    if (row + 2u < rows) nxt = load_row_streaming(rowp + (size_t)(row + 2u) * a.seg);
+                    q[0] = fetch(e.x & 0xffffu); q[1] = fetch(e.x >> 16);
+                    q[2] = fetch(e.y & 0xffffu); q[3] = fetch(e.y >> 16);
+                    q[4] = fetch(e.z & 0xffffu); q[5] = fetch(e.z >> 16);
+                    q[6] = fetch(e.w & 0xffffu); q[7] = fetch(e.w >> 16);
+                }
+#pragma unroll
+                for (int m = 0; m < 8; m++) add(c[m]);
+            }
+#else
             for (uint32_t row = 0; row < rows; row++) {
                 const uint4 e = nxt;
                 if (row + 1u < rows) nxt = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
-                add(e.x & 0xffffu);
-                add(e.x >> 16);
-                add(e.y & 0xffffu);
-                add(e.y >> 16);
-                add(e.z & 0xffffu);
-                add(e.z >> 16);
-                add(e.w & 0xffffu);
-                add(e.w >> 16);
+                add(fetch(e.x & 0xffffu));
+                add(fetch(e.x >> 16));
+                add(fetch(e.y & 0xffffu));
+                add(fetch(e.y >> 16));
+                add(fetch(e.z & 0xffffu));
+                add(fetch(e.z >> 16));
+                add(fetch(e.w & 0xffffu));
+                add(fetch(e.w >> 16));
             }
+#endif
         } else {
             const uint4 own = cur[i];
             const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;

@@ -67,6 +67,16 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #ifndef VLJ_GATHER_AHEAD
 #define VLJ_GATHER_AHEAD 0
 #endif
+// Cell tiles of the step kernel (tile_step_kernel): 1 stages f32 offsets
+// from the brick's centre instead of the encoded words (the separation is a
+// plain f32 difference, not the same bits as the list kernels); 1 reads the
+// next list row's neighbours while computing this row's pairs.
+#ifndef VLJ_TILE_F32
+#define VLJ_TILE_F32 0
+#endif
+#ifndef VLJ_TILE_PIPE
+#define VLJ_TILE_PIPE 0
+#endif
 constexpr int kForceThreads = 128;
 constexpr uint32_t kDenseCell = 8;  // particles in a cell the list build takes first
 // In a box under five cells wide on some axis (a batched replica) a cell
