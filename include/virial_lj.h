@@ -329,8 +329,10 @@ VLJ_API vlj_status vlj_debug_kernel_time(vlj_sim *sim, double *total_ms, uint64_
 /* FP32 FMA throughput of the current device in TFLOP/s (a calibration kernel
  * of independent FMA chains on every SM). */
 VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
-/* Cell tiles of the step kernel (single boxes of four or more particles per
- * cell on average): 0 switches the step kernel back to per-particle gathers
+/* Cell tiles of the step kernel: single boxes of four or more particles per
+ * cell on average created with the environment variable VLJ_TILES=1 (off by
+ * default: slower than the per-particle gathers on the workloads measured).
+ * set_tiles(sim, 0) switches the step kernel back to per-particle gathers
  * from the slot list (same trajectory to the bit); tile_info gives the
  * bricks per x-row, the bricks in all, the tile capacity (particles a block
  * stages) and the threads per block (all 0 without tiles). read_tile_lists

@@ -19,6 +19,18 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def tiles_on():
+    # cell tiles are opt-in at creation (VLJ_TILES=1)
+    before = os.environ.get("VLJ_TILES")
+    os.environ["VLJ_TILES"] = "1"
+    yield
+    if before is None:
+        del os.environ["VLJ_TILES"]
+    else:
+        os.environ["VLJ_TILES"] = before
+
+
 def tile_of_brick(grid, cells, cols, index):
     """The slots a brick's tile holds, in tile order (nine x-rows dz, dy =
     -1..1 over the brick's cells and one more each side, or the whole row)."""
