@@ -91,6 +91,11 @@ typedef struct {
     uint32_t list_overflow; /* 0, or the largest neighbour count that did not fit */
     double thermostat_energy;
     uint32_t condensed;
+    /* No reference counterpart: the list capacity (entries per particle) the
+     * measurement ran with, and how many times it has grown since creation
+     * (vlj_set_list_growth). */
+    uint32_t list_capacity;
+    uint32_t list_grows;
 } vlj_measurement;
 
 /* lennard_jones.rs:133-147: one slab's averages per sample */
@@ -179,6 +184,22 @@ VLJ_API vlj_status vlj_set_temperature(vlj_sim *sim, double temperature);
 VLJ_API vlj_status vlj_set_heat_exchange(vlj_sim *sim, const vlj_heat_exchange *exchange);
 /* *has = 0 when no exchange is set. */
 VLJ_API vlj_status vlj_heat_flux(const vlj_sim *sim, int *has, double *flux);
+/* List capacity recovery (no reference counterpart; on by default). The
+ * capacity starts at the reference's rule (twice the mean neighbour count
+ * within cutoff + skin, plus 32; lennard_jones.rs:471-474), which a dense
+ * region of a mostly dilute box (a liquid slab) can exceed. The reference
+ * only reports that through list_overflow, and the particles concerned lose
+ * pairs until the next rebuild. With growth on, when a list overflows the
+ * host raises that box's capacity to 1.25 x the largest count (rounded up to
+ * a multiple of 8), reallocates the lists and rebuilds them: vlj_run checks
+ * after its steps, vlj_measure_now grows and measures again (so the
+ * measurement it returns has every pair), a measurement read by vlj_poll
+ * schedules the grow for the next vlj_step. Each grow is counted in
+ * vlj_measurement.list_grows; a build that overflows at creation grows the
+ * lists before the first forces. 0 restores the reference's report-only
+ * behaviour (from creation on when the environment sets
+ * VLJ_LIST_GROWTH=0). */
+VLJ_API vlj_status vlj_set_list_growth(vlj_sim *sim, int on);
 /* No reference counterpart (the reference bins only when the lists rebuild):
  * with on != 0, rebuild the cell grid (bin, scan, scatter, per-cell sort) on
  * every step, the Verlet lists still on the skin / 2 trigger. Same trajectory

@@ -214,6 +214,9 @@ vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_encode(s->arena, s->stream));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
+    // lists that overflowed on the first build grow before the first forces
+    bool grew = false;
+    TRY(sim_grow_lists(s, &grew));
     if (s->canonical()) {
         // the thermostat starts at rest (xi = eta = 0) from the given
         // velocities; the first forces are recorded for the first half kick
@@ -250,6 +253,8 @@ vlj_measurement decode(const vlj_sim* s, const Readback& r, uint64_t step) {
     m.list_rebuilds = r.ctrl.rebuilds;
     m.list_overflow = r.ctrl.overflow;
     m.condensed = (uint32_t)std::llround(value(r.slots[6]));
+    m.list_capacity = s->box.capacity;
+    m.list_grows = s->list_grows;
     // lennard_jones.rs:1235-1241: Q xi^2 / 2 + g k T eta
     m.thermostat_energy = s->nose_hoover
         ? 0.5 * s->box.nh_q * r.nh.xi_m * r.nh.xi_m + s->box.nh_gkt * r.nh.eta_m : 0.0;
@@ -329,6 +334,7 @@ vlj_status vlj_create(const vlj_particle* particles, size_t count, const vlj_set
         return fail(VLJ_INVALID_ARG, "Nose-Hoover needs at least two particles");
 
     vlj_sim* s = new vlj_sim();
+    s->list_growth = list_growth_default();
     s->settings = *settings;
     s->n = (uint32_t)count;
     s->shifted_force = settings->shifted_force != 0;
@@ -359,6 +365,10 @@ vlj_status vlj_destroy(vlj_sim* sim) {
 
 vlj_status vlj_step(vlj_sim* s, uint32_t steps) {
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (s->grow_pending) {
+        bool grew = false;
+        TRY(sim_grow_lists(s, &grew));
+    }
     TRY(sim_enqueue_steps(s, steps));
     s->steps += steps;
     return VLJ_OK;
@@ -372,7 +382,9 @@ vlj_status vlj_run(vlj_sim* s, uint64_t steps) {
         steps -= batch;
     }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    return check_fault(s);
+    TRY(check_fault(s));
+    bool grew = false;
+    return sim_grow_lists(s, &grew);
 }
 
 vlj_status vlj_measure(vlj_sim* s, int* accepted) {
@@ -406,7 +418,9 @@ vlj_status vlj_poll(vlj_sim* s, vlj_measurement* out, size_t capacity, size_t* w
     size_t n = 0;
     for (auto& r : ready) {
         if (n >= capacity || !out) break;
-        out[n++] = decode(s, s->ring[r.second], r.first);
+        out[n] = decode(s, s->ring[r.second], r.first);
+        if (out[n].list_overflow && s->list_growth) s->grow_pending = true;
+        n++;
         s->ring_busy[r.second] = false;
     }
     *written = n;
@@ -424,7 +438,14 @@ vlj_status vlj_measure_now(vlj_sim* s, vlj_measurement* out) {
     TRY(vlj_poll(s, buf, kRing, &n));
     if (n == 0) return fail(VLJ_CUDA_ERROR, "the measurement did not finish");
     *out = buf[n - 1];
-    return check_fault(s);
+    TRY(check_fault(s));
+    if (out->list_overflow && s->list_growth) {
+        // lists that dropped pairs: grow them, rebuild, measure again
+        bool grew = false;
+        TRY(sim_grow_lists(s, &grew));
+        if (grew) return vlj_measure_now(s, out);
+    }
+    return VLJ_OK;
 }
 
 vlj_status vlj_read_particles(vlj_sim* s, vlj_particle* out) {
@@ -592,6 +613,13 @@ vlj_status vlj_set_grid_every_step(vlj_sim* s, int on) {
                              cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->grid_every_step = want;
+    return VLJ_OK;
+}
+
+vlj_status vlj_set_list_growth(vlj_sim* s, int on) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    s->list_growth = on != 0;
+    if (!s->list_growth) s->grow_pending = false;
     return VLJ_OK;
 }
 
@@ -1247,6 +1275,77 @@ vlj_status sim_flush_heat(vlj_sim* s) {
     TRY(lists_now(s));
     CUDA_TRY(launch_heat_current(s->arena, s->shifted_force, s->series_samples - 1u, s->stream));
     return VLJ_OK;
+}
+
+// Replaces device allocation `old` (one of s->allocations) by a new one of
+// `bytes` bytes.
+static vlj_status realloc_device(vlj_sim* s, void** ptr, size_t bytes) {
+    void* q = nullptr;
+    CUDA_TRY(cudaMalloc(&q, bytes));
+    CUDA_TRY(cudaMemset(q, 0, bytes));
+    for (void*& p : s->allocations)
+        if (p == *ptr) {
+            cudaFree(p);
+            p = q;
+            *ptr = q;
+            return VLJ_OK;
+        }
+    cudaFree(q);
+    return fail(VLJ_CUDA_ERROR, "list allocation not found");
+}
+
+bool list_growth_default() {
+    const char* env = std::getenv("VLJ_LIST_GROWTH");
+    return !(env && env[0] == '0');
+}
+
+vlj_status sim_grow_lists(vlj_sim* s, bool* grew) {
+    *grew = false;
+    s->grow_pending = false;
+    if (!s->list_growth) return VLJ_OK;
+    Arena& a = s->arena;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    std::vector<Control> c(a.nboxes);
+    CUDA_TRY(cudaMemcpy(c.data(), a.ctrl, sizeof(Control) * c.size(), cudaMemcpyDeviceToHost));
+    const bool batched = !s->replicas.empty();
+    std::vector<Box> single;
+    if (!batched) single.push_back(s->box);
+    std::vector<Box>& boxes = batched ? s->replicas : single;
+    uint32_t old_max = 0, new_max = 0;
+    bool any = false;
+    for (size_t b = 0; b < boxes.size(); b++) {
+        old_max = std::max(old_max, boxes[b].capacity);
+        if (c[b].overflow > boxes[b].capacity) {
+            const uint32_t want = (uint32_t)std::ceil(1.25 * (double)c[b].overflow);
+            boxes[b].capacity = (want + 7u) / 8u * 8u;
+            c[b].overflow = 0u;
+            c[b].forced = 1u;
+            any = true;
+        }
+        new_max = std::max(new_max, boxes[b].capacity);
+    }
+    if (!any) return VLJ_OK;
+    const size_t seg = a.seg;
+    if ((new_max + 3u) / 4u > (old_max + 3u) / 4u) {
+        TRY(realloc_device(s, reinterpret_cast<void**>(&a.list),
+                           sizeof(uint32_t) * seg * 4 * ((new_max + 3) / 4)));
+        TRY(make_list_map(a, (new_max + 3) / 4, &s->list_map));
+    }
+    if (a.list16 && (new_max + 7u) / 8u > (old_max + 7u) / 8u)
+        TRY(realloc_device(s, reinterpret_cast<void**>(&a.list16),
+                           sizeof(uint16_t) * seg * 8 * ((new_max + 7) / 8)));
+    if (!batched) s->box = boxes[0];
+    CUDA_TRY(cudaMemcpy(const_cast<Box*>(a.boxes), boxes.data(), sizeof(Box) * boxes.size(),
+                        cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(a.ctrl, c.data(), sizeof(Control) * c.size(), cudaMemcpyHostToDevice));
+    // the captured graphs hold the old arena
+    sim_drop_step_graphs(s);
+    if (s->graph_lists) cudaGraphExecDestroy(s->graph_lists);
+    s->graph_lists = nullptr;
+    s->list_grows += 1;
+    *grew = true;
+    // the forced rebuild now, so what follows reads full lists
+    return lists_now(s);
 }
 
 void sim_drop_step_graphs(vlj_sim* s) {

@@ -108,6 +108,8 @@ vlj_measurement decode(const vlj_sim* s, const Box& bx, const long long* slots,
     m.list_rebuilds = c.rebuilds;
     m.list_overflow = c.overflow;
     m.condensed = (uint32_t)std::llround(value(slots[6]));
+    m.list_capacity = bx.capacity;
+    m.list_grows = s->list_grows;
     return m;
 }
 
@@ -159,6 +161,7 @@ vlj_status vlj_batch_create(const vlj_replica_desc* replicas, size_t count, doub
 
     vlj_batch* bt = new vlj_batch();
     vlj_sim* s = new vlj_sim();
+    s->list_growth = list_growth_default();
     bt->sim = s;
     std::memset(&s->settings, 0, sizeof s->settings);
     s->settings.cutoff = cutoff;
@@ -186,9 +189,14 @@ vlj_status vlj_batch_create(const vlj_replica_desc* replicas, size_t count, doub
         cudaError_t e = launch_decide(s->arena, s->stream, 0);
         if (e == cudaSuccess) e = launch_encode(s->arena, s->stream);
         if (e == cudaSuccess) e = launch_rebuild(s->arena, s->stream);
+        // lists that overflowed on the first build grow before the first forces
+        bool grew = false;
+        if (e == cudaSuccess) st = sim_grow_lists(s, &grew);
+        if (st != VLJ_OK) e = cudaErrorUnknown;
         if (e == cudaSuccess) e = launch_prime(s->arena, s->list_map, s->shifted_force, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        if (e != cudaSuccess) st = fail(VLJ_CUDA_ERROR, "first lists: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess && st == VLJ_OK)
+            st = fail(VLJ_CUDA_ERROR, "first lists: %s", cudaGetErrorString(e));
     }
     if (st == VLJ_OK) st = check_fault(s);
     if (st != VLJ_OK) {
@@ -206,6 +214,10 @@ vlj_status vlj_batch_destroy(vlj_batch* batch) {
 
 vlj_status vlj_batch_step(vlj_batch* bt, uint32_t steps) {
     if (!bt) return fail(VLJ_INVALID_ARG, "batch is null");
+    if (bt->sim->grow_pending) {
+        bool grew = false;
+        TRY(sim_grow_lists(bt->sim, &grew));
+    }
     TRY(sim_enqueue_steps(bt->sim, steps));
     bt->sim->steps += steps;
     return VLJ_OK;
@@ -219,7 +231,9 @@ vlj_status vlj_batch_run(vlj_batch* bt, uint64_t steps) {
         steps -= chunk;
     }
     CUDA_TRY(cudaStreamSynchronize(bt->sim->stream));
-    return check_fault(bt->sim);
+    TRY(check_fault(bt->sim));
+    bool grew = false;
+    return sim_grow_lists(bt->sim, &grew);
 }
 
 vlj_status vlj_batch_measure(vlj_batch* bt, vlj_measurement* out) {
@@ -233,6 +247,14 @@ vlj_status vlj_batch_measure(vlj_batch* bt, vlj_measurement* out) {
                              cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     TRY(check_fault(s));
+    bool overflow = false;
+    for (size_t r = 0; r < boxes; r++) overflow = overflow || bt->ctrl[r].overflow != 0u;
+    if (overflow && s->list_growth) {
+        // lists that dropped pairs: grow them, rebuild, measure again
+        bool grew = false;
+        TRY(sim_grow_lists(s, &grew));
+        if (grew) return vlj_batch_measure(bt, out);
+    }
     for (size_t r = 0; r < boxes; r++)
         out[r] = decode(s, s->replicas[r], bt->accum + kSlots * r, bt->ctrl[r]);
     return VLJ_OK;

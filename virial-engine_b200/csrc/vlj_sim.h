@@ -43,6 +43,9 @@ struct vlj_sim {
     bool canonical() const { return nose_hoover || exchange; }
     bool grid_every_step = false;  // bin, scan, scatter, sort every step; lists on the trigger
     bool tiles_on = true;  // the step kernel stages cell tiles (when the box has them)
+    bool list_growth = true;   // grow the list capacity when a list overflows
+    bool grow_pending = false; // a polled measurement showed an overflow
+    uint32_t list_grows = 0;   // capacity grows so far
     vlj::Box box{};
     // batched: one Box per replica, in slot order (empty for a single box)
     std::vector<vlj::Box> replicas;
@@ -94,6 +97,13 @@ vlj_status check_fault(vlj_sim* s);
 vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps);
 // Takes a pending heat-current sample now, with the sampling kernel.
 vlj_status sim_flush_heat(vlj_sim* s);
+// With list growth on and a list overflowed since the last build: raise the
+// capacity of every box that overflowed, reallocate the lists, drop the
+// captured graphs and force a rebuild (waits). *grew says whether it did.
+vlj_status sim_grow_lists(vlj_sim* s, bool* grew);
+// List growth at creation: on, unless the environment sets VLJ_LIST_GROWTH=0
+// (the reference's report-only behaviour from the first build on).
+bool list_growth_default();
 // Drops the captured step graphs (their shape changed).
 void sim_drop_step_graphs(vlj_sim* s);
 // The decision and, when due, the rebuild as one graph launch.

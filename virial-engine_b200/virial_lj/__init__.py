@@ -157,12 +157,14 @@ class Measurement:
     list_overflow: int
     thermostat_energy: float
     condensed: int
+    list_capacity: int = 0  # list entries per particle the measurement ran with
+    list_grows: int = 0     # capacity grows since creation (set_list_growth)
 
     @staticmethod
     def _from(m):
         return Measurement(m.step, m.time, m.kinetic, m.potential, m.virial, list(m.momentum),
                            m.count, m.volume, m.list_rebuilds, m.list_overflow,
-                           m.thermostat_energy, m.condensed)
+                           m.thermostat_energy, m.condensed, m.list_capacity, m.list_grows)
 
     def energy(self):
         return self.kinetic + self.potential
@@ -401,6 +403,11 @@ class LennardJones:
         has, f = C.c_int(), C.c_double()
         _check(_lib.vlj_heat_flux(self._h, C.byref(has), C.byref(f)))
         return f.value if has.value else None
+
+    def set_list_growth(self, on):
+        """Grow the list capacity when a list overflows (on by default; off is
+        the reference's report-only behaviour)."""
+        _check(_lib.vlj_set_list_growth(self._h, int(bool(on))))
 
     def set_grid_every_step(self, on):
         """Rebuild the cell grid on every step as well (the lists still on the

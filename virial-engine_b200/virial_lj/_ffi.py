@@ -28,7 +28,8 @@ class Measurement(C.Structure):
                 ("potential", C.c_double), ("virial", C.c_double), ("momentum", C.c_double * 3),
                 ("count", C.c_uint32), ("volume", C.c_double), ("list_rebuilds", C.c_uint32),
                 ("list_overflow", C.c_uint32), ("thermostat_energy", C.c_double),
-                ("condensed", C.c_uint32)]
+                ("condensed", C.c_uint32), ("list_capacity", C.c_uint32),
+                ("list_grows", C.c_uint32)]
 
 
 class Slab(C.Structure):
@@ -84,6 +85,7 @@ SIGNATURES = {
     "vlj_set_heat_exchange": [_vp, _P(HeatExchange)],
     "vlj_heat_flux": [_vp, _P(C.c_int), _P(C.c_double)],
     "vlj_set_grid_every_step": [_vp, C.c_int],
+    "vlj_set_list_growth": [_vp, C.c_int],
     "vlj_sample_profile": [_vp],
     "vlj_clear_profile": [_vp],
     "vlj_read_profile": [_vp, _P(Slab), _P(C.c_double), _P(C.c_uint64)],
