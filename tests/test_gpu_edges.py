@@ -60,13 +60,24 @@ def test_mostly_empty_cells(gpu, O):
 
 def test_list_overflow_is_reported(gpu):
     # 216 particles packed 0.2 apart at a mean density of 0.125: far more
-    # neighbours than the lists hold; reported, and nothing is written past them
+    # neighbours than the lists hold. With list growth off (the reference's
+    # behaviour) the overflow is reported and nothing is written past the
+    # lists; with it on (the default) the lists grow to hold all 215.
+    import os
     g = np.arange(6) * 0.2 + 3.0
     pos = np.array([[x, y, z] for x in g for y in g for z in g])
-    sim = gpu.LennardJones(gpu.particles(pos), settings(gpu, 12.0))
+    os.environ["VLJ_LIST_GROWTH"] = "0"
+    try:
+        sim = gpu.LennardJones(gpu.particles(pos), settings(gpu, 12.0))
+    finally:
+        del os.environ["VLJ_LIST_GROWTH"]
     cap = sim.grid_info().capacity
     m = sim.measure_now()
-    assert m.list_overflow == 215 > cap
+    assert m.list_overflow == 215 > cap and m.list_grows == 0
+    sim = gpu.LennardJones(gpu.particles(pos), settings(gpu, 12.0))
+    m = sim.measure_now()
+    assert m.list_overflow == 0 and m.list_grows == 1
+    assert m.list_capacity == sim.grid_info().capacity >= 215 > cap
 
 
 def test_non_finite_input_is_refused(gpu):
