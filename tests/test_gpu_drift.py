@@ -8,8 +8,11 @@ lattice at T = 2 (seed 13), force-shifted cutoff 2.5, constant energy, dt
 oracle (oracle/dfpath.c: double-float state, f32 pair arithmetic on packed
 positions, df64 sums). Here both paths, and the f64 engine beside them, run
 the same starts side by side: the reference's drift configuration and the
-small plain workload (1000 atoms at rho 0.8442, T 0.72, seeds 1, 2, 3, both
-cutoff styles, 1000 steps). Each drift is the relative change of total
+small plain workload (1000 atoms at rho 0.8442, T 0.72, both cutoff styles,
+1000 steps). The reference's lattice seeds its generator with seed | 1
+(lennard_jones.rs:1409), so seeds 2 and 3 give the same start: the distinct
+odd seeds 1, 3, ..., 11 stand in for "seeds 1, 2, 3". Each drift is the
+relative change of total
 energy over the run. Over these runs the trajectories decorrelate (the
 dynamics is chaotic), so each path's drift is a sample: the CUDA path must
 be no worse than the double-float path, within the double-float path's own
@@ -59,15 +62,15 @@ def check(rows, label):
 @pytest.mark.parametrize("shifted_force", [False, True])
 def test_drift_small_plain_workload(gpu, O, shifted_force):
     rows = [drifts(gpu, O, 1000, 0.8442, 0.72, seed, shifted_force, 0.005, 1000)
-            for seed in (1, 2, 3)]
+            for seed in (1, 3, 5, 7, 9, 11)]
     check(rows, f"1000 atoms, rho 0.8442, T 0.72, dt 0.005, 1000 steps, "
                 f"{'force' if shifted_force else 'truncated'}-shifted")
 
 
 def test_drift_reference_study_configuration(gpu, O):
     # lj_dt_study.rs: 4096 molecules, density 0.1, T = 2, force-shifted,
-    # dt 0.004, 40 time units; seed 13 is the reference's, 14 and 15 give the spread
-    rows = [drifts(gpu, O, 4096, 0.1, 2.0, seed, True, 0.004, 10_000) for seed in (13, 14, 15)]
+    # dt 0.004, 40 time units; seed 13 is the reference's, 15 and 17 give the spread
+    rows = [drifts(gpu, O, 4096, 0.1, 2.0, seed, True, 0.004, 10_000) for seed in (13, 15, 17)]
     check(rows, "4096 molecules, rho 0.1, T 2, force-shifted, dt 0.004, 40 time units "
                 "(the reference measured +5.0e-5 with seed 13)")
     # the reference's own figure sets the scale: every path within 4x of it
