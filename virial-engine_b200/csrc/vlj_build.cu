@@ -46,6 +46,11 @@ namespace vlj {
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
 #endif
+// 1: in boxes of five or more cells a side, the test takes two home
+// particles at a time
+#ifndef VLJ_BUILD_PAIRS
+#define VLJ_BUILD_PAIRS 0
+#endif
 constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
 constexpr int kRound = VLJ_BUILD_ROUND;
 constexpr int kStage = VLJ_BUILD_STAGE;
@@ -348,6 +353,58 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                                        e_tix);
                         if (lane == h) found += (uint32_t)__popc(m);
                     };
+#if VLJ_BUILD_PAIRS
+                    if (wide) {
+                        // two home particles at a time: their tests are
+                        // independent, so each one's dependent chain of
+                        // arithmetic, votes and stores fills the other's gaps
+                        const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
+                                    ez = __uint_as_float(e.z);
+                        for (uint32_t h = 0; h < homes; h += 2) {
+                            const bool two = h + 1u < homes;
+                            const uint32_t h1 = two ? h + 1u : h;
+                            const uint4 pa = s_home[warp][h], pb = s_home[warp][h1];
+                            const float ax = ex - __uint_as_float(pa.x), bx_ = ex - __uint_as_float(pb.x);
+                            const float ay = ey - __uint_as_float(pa.y), by = ey - __uint_as_float(pb.y);
+                            const float az = ez - __uint_as_float(pa.z), bz = ez - __uint_as_float(pb.z);
+                            const float ra = ax * ax + ay * ay + az * az;
+                            const float rb = bx_ * bx_ + by * by + bz * bz;
+                            const bool near_a = valid && ra < pre_r2 && e.w != pa.w;
+                            const bool near_b = two && valid && rb < pre_r2 && e.w != pb.w;
+                            bool take_a = near_a && ra < acc_r2;
+                            bool take_b = near_b && rb < acc_r2;
+                            if (near_a && !take_a) take_a = ref_test(a, bx, pa.w, e.w, s_q510);
+                            if (near_b && !take_b) take_b = ref_test(a, bx, pb.w, e.w, s_q510);
+                            const unsigned ma = __ballot_sync(0xffffffffu, take_a);
+                            const unsigned mb = __ballot_sync(0xffffffffu, take_b);
+                            if ((ma | mb) == 0u) continue;
+                            const uint32_t ka = __shfl_sync(0xffffffffu, found, h) +
+                                                (uint32_t)__popc(ma & below);
+                            const uint32_t kb = __shfl_sync(0xffffffffu, found, h1) +
+                                                (uint32_t)__popc(mb & below);
+                            store_if(take_a && ka < cap,
+                                     a.list + ((unsigned long long)(ka >> 2) * row_stride +
+                                               (pa.w * 4u + (ka & 3u))),
+                                     e.w);
+                            store_if(take_b && kb < cap,
+                                     a.list + ((unsigned long long)(kb >> 2) * row_stride +
+                                               (pb.w * 4u + (kb & 3u))),
+                                     e.w);
+                            if (tiles) {
+                                store16_if(take_a && ka < cap,
+                                           a.list16 + ((unsigned long long)(ka >> 3) * row16_stride +
+                                                       ((h0 + h) * 8u + (ka & 7u))),
+                                           e_tix);
+                                store16_if(take_b && kb < cap,
+                                           a.list16 + ((unsigned long long)(kb >> 3) * row16_stride +
+                                                       ((h0 + h1) * 8u + (kb & 7u))),
+                                           e_tix);
+                            }
+                            if (lane == h) found += (uint32_t)__popc(ma);
+                            if (two && lane == h1) found += (uint32_t)__popc(mb);
+                        }
+                    } else
+#else
                     if (wide) {
                         const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
                                     ez = __uint_as_float(e.z);
@@ -358,7 +415,9 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                             const float dz = ez - __uint_as_float(hp.z);
                             settle(h, hp.w, dx * dx + dy * dy + dz * dz);
                         }
-                    } else {
+                    } else
+#endif
+                    {
                         for (uint32_t h = 0; h < homes; h++) {
                             const uint4 hp = s_home[warp][h];
                             settle(h, hp.w, encoded_r2(e, hp, dec));
