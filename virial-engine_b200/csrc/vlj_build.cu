@@ -49,7 +49,7 @@ namespace vlj {
 // 1: in boxes of five or more cells a side, the test takes two home
 // particles at a time
 #ifndef VLJ_BUILD_PAIRS
-#define VLJ_BUILD_PAIRS 0
+#define VLJ_BUILD_PAIRS 1
 #endif
 constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
 constexpr int kRound = VLJ_BUILD_ROUND;
