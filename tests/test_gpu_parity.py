@@ -281,9 +281,10 @@ def test_grid_every_step_keeps_the_trajectory(gpu):
     for sim in (plain, every, direct):
         sim.run(200)
     k_plain, k_every = plain.kernels_executed() - k_plain, every.kernels_executed() - k_every
-    # a step kernel per step, a decide per graph launch (12 of 16 steps, 8 of
-    # one), six more per rebuild
-    rebuilds, rest = divmod(k_plain - 200 - 20, 6)
+    # a step kernel per step, a decide per 16-step graph launch (12), one for
+    # the first of the 8 one-step graphs (each of them takes the next one's
+    # decision), six more per rebuild
+    rebuilds, rest = divmod(k_plain - 200 - 13, 6)
     assert rest == 0 and rebuilds > 0
     ms = [sim.measure_now() for sim in (plain, every, direct)]
     assert ms[0].list_rebuilds - r0 >= rebuilds
@@ -297,3 +298,31 @@ def test_grid_every_step_keeps_the_trajectory(gpu):
     assert np.array_equal(g0["counts"], g1["counts"]) and np.array_equal(g0["lists"], g1["lists"])
     # bin, scan, scatter and sort also on every step without a rebuild
     assert k_every - k_plain == 4 * (200 - rebuilds)
+
+
+def test_single_steps_carry_their_decisions(gpu):
+    # one-step graphs take the next step's rebuild decision in their step
+    # kernel and skip their decide kernel while it stands; measurements,
+    # forced rebuilds and chunks in between must leave the trajectory as
+    # direct launches (a decide kernel every step) make it
+    p, L = gpu.lattice_fcc(10, 0.8442, 1.5, 5)
+    st = gpu.Settings([L] * 3, dt=0.005, shifted_force=True, thermostat=gpu.Langevin(1.5, 1.0, 4))
+    out = []
+    for graphs in (True, False):
+        sim = gpu.LennardJones(p, st)
+        sim.set_graphs(graphs)
+        k0 = sim.kernels_executed()
+        for k in range(120):
+            sim.step(1)
+            if k % 37 == 5:
+                sim.measure_now()
+            if k == 70:
+                sim.force_rebuild()
+            if k == 90:
+                sim.step(16)
+        m = sim.measure_now()
+        out.append((sim.read_particles().tobytes(), m.potential, m.virial, m.list_rebuilds,
+                    sim.kernels_executed() - k0))
+    assert out[0][:4] == out[1][:4]
+    assert out[0][3] > 10  # rebuilds on the way
+    assert out[0][4] < out[1][4]  # the graphs launched fewer decide kernels

@@ -198,6 +198,7 @@ vlj_status upload_particles(vlj_sim* s, const vlj_particle* p, size_t count) {
 }
 
 vlj_status lists_now(vlj_sim* s) {
+    s->one_ready = false;
     if (s->use_graphs && !s->timing) return sim_launch_lists_graph(s);
     CUDA_TRY(launch_decide(s->arena, s->stream, 0));
     CUDA_TRY(launch_rebuild(s->arena, s->stream));
@@ -207,6 +208,7 @@ vlj_status lists_now(vlj_sim* s) {
 // Fresh state from `p`: forced rebuild, then the first forces turn the given
 // velocities into ones half a kick behind (lennard_jones.rs:1080-1089).
 vlj_status restart(vlj_sim* s, const vlj_particle* p, size_t count) {
+    s->one_ready = false;
     TRY(upload_particles(s, p, count));
     uint32_t one = 1u;
     CUDA_TRY(cudaMemcpyAsync(&s->arena.ctrl[0].forced, &one, sizeof one, cudaMemcpyHostToDevice,
@@ -287,6 +289,7 @@ vlj_status enqueue_measure(vlj_sim* s, bool canonical, int slot) {
 vlj_sim::~vlj_sim() {
     if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
     if (graph_one) cudaGraphExecDestroy(graph_one);
+    if (graph_one_tmpl) cudaGraphDestroy(graph_one_tmpl);
     if (graph_one_heat) cudaGraphExecDestroy(graph_one_heat);
     if (graph_lists) cudaGraphExecDestroy(graph_lists);
     if (capture_stream) cudaStreamDestroy(capture_stream);
@@ -1131,22 +1134,33 @@ static cudaError_t launch_step_tail(vlj_sim* s, cudaStream_t cs) {
 // step kernel, chained (canonical velocities: begin -> decide -> IF{...} ->
 // canon_force [-> hex_apply]). The decide kernel sets the condition on the device, so a step
 // with no rebuild launches no rebuild kernel at all.
+// With `keep`, a graph of one step whose step kernel takes the next step's
+// decision and sets this graph's own condition for its next launch: the
+// template graph and the decide node come back through *keep and
+// *decide_node (the caller disables the node while that decision stands).
 static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out,
-                              bool heat = false) {
+                              bool heat = false, cudaGraph_t* keep = nullptr,
+                              cudaGraphNode_t* decide_node = nullptr) {
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaGraphCreate(&g, 0));
     struct Guard {
         cudaGraph_t g;
-        ~Guard() { cudaGraphDestroy(g); }
+        ~Guard() {
+            if (g) cudaGraphDestroy(g);
+        }
     } guard{g};
+    const bool self_fold = keep && count == 1 && !s->canonical();
     cudaStream_t cs = s->capture_stream;
     const auto mode = cudaStreamCaptureModeThreadLocal;
     // one conditional per step; with the fused step kernel, step k's kernel
     // takes step k + 1's decision, so only the first step launches decide
     const bool fold = !s->canonical();
     std::vector<cudaGraphConditionalHandle> h(count);
+    // a condition that a step kernel sets for the graph's next launch keeps
+    // its value between launches
     for (uint32_t k = 0; k < count; k++)
-        CUDA_TRY(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&h[k], g, 0,
+                                                  self_fold ? 0u : cudaGraphCondAssignDefault));
     cudaGraphNode_t prev = nullptr;
     for (uint32_t k = 0; k < count; k++) {
         cudaGraphNode_t n_decide = nullptr, n_cond = nullptr;
@@ -1157,6 +1171,7 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out,
             if (s->canonical()) e = launch_begin(s->arena, cs);
             if (e == cudaSuccess) e = launch_decide(s->arena, cs, h[k]);
             TRY(end_capture(cs, e, &n_decide));
+            if (self_fold && decide_node) *decide_node = n_decide;
         } else {
             n_decide = prev;  // the previous step kernel decided
         }
@@ -1179,12 +1194,18 @@ static vlj_status build_graph(vlj_sim* s, uint32_t count, cudaGraphExec_t* out,
         cudaError_t e;
         if (fold)
             e = launch_step(step_arena(s), s->list_map, s->shifted_force, cs,
-                            k + 1 < count ? (unsigned long long)h[k + 1] : 0ull, heat && k == 0);
+                            k + 1 < count ? (unsigned long long)h[k + 1]
+                                          : (self_fold ? (unsigned long long)h[k] : 0ull),
+                            heat && k == 0);
         else
             e = launch_step_tail(s, cs);
         TRY(end_capture(cs, e, &prev));
     }
     CUDA_TRY(cudaGraphInstantiate(out, g, 0));
+    if (self_fold) {
+        *keep = g;
+        guard.g = nullptr;
+    }
     return VLJ_OK;
 }
 
@@ -1218,6 +1239,7 @@ vlj_status sim_launch_lists_graph(vlj_sim* s) {
 }
 
 static vlj_status step_direct(vlj_sim* s, bool heat = false) {
+    s->one_ready = false;
     if (s->canonical()) {
         CUDA_TRY(launch_begin(s->arena, s->stream));
         CUDA_TRY(launch_decide(s->arena, s->stream, 0));
@@ -1253,6 +1275,7 @@ vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
         } else {
             if (!s->graph_one_heat) TRY(build_graph(s, 1, &s->graph_one_heat, true));
             CUDA_TRY(cudaGraphLaunch(s->graph_one_heat, s->stream));
+            s->one_ready = false;
         }
         s->heat_pending = false;
         steps -= 1;
@@ -1262,10 +1285,28 @@ vlj_status sim_enqueue_steps(vlj_sim* s, uint32_t steps) {
         return VLJ_OK;
     }
     if (!s->graph_chunk) TRY(build_graph(s, kGraphChunk, &s->graph_chunk));
-    if (!s->graph_one) TRY(build_graph(s, 1, &s->graph_one));
-    for (; steps >= kGraphChunk; steps -= kGraphChunk)
+    if (!s->graph_one) {
+        s->one_decide = nullptr;
+        TRY(build_graph(s, 1, &s->graph_one, false, &s->graph_one_tmpl, &s->one_decide));
+        s->one_decide_on = true;
+        s->one_ready = false;
+    }
+    for (; steps >= kGraphChunk; steps -= kGraphChunk) {
         CUDA_TRY(cudaGraphLaunch(s->graph_chunk, s->stream));
-    for (; steps > 0; steps--) CUDA_TRY(cudaGraphLaunch(s->graph_one, s->stream));
+        s->one_ready = false;  // the chunk's last step leaves the decision open
+    }
+    for (; steps > 0; steps--) {
+        if (s->one_decide) {
+            // the previous step (graph_one's) decided this one already
+            const bool need = !s->one_ready;
+            if (need != s->one_decide_on) {
+                CUDA_TRY(cudaGraphNodeSetEnabled(s->graph_one, s->one_decide, need ? 1u : 0u));
+                s->one_decide_on = need;
+            }
+        }
+        CUDA_TRY(cudaGraphLaunch(s->graph_one, s->stream));
+        s->one_ready = s->one_decide != nullptr;
+    }
     return VLJ_OK;
 }
 
@@ -1351,6 +1392,10 @@ vlj_status sim_grow_lists(vlj_sim* s, bool* grew) {
 void sim_drop_step_graphs(vlj_sim* s) {
     if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
     if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
+    if (s->graph_one_tmpl) cudaGraphDestroy(s->graph_one_tmpl);
+    s->graph_one_tmpl = nullptr;
+    s->one_decide = nullptr;
+    s->one_ready = false;
     if (s->graph_one_heat) cudaGraphExecDestroy(s->graph_one_heat);
     s->graph_chunk = s->graph_one = s->graph_one_heat = nullptr;
 }

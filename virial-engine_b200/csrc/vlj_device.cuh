@@ -32,6 +32,13 @@ __device__ __forceinline__ void count_kernel(const Arena& a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.glob->kernels, 1ull);
 }
 
+// A step starts: the decision taken for it (if a step kernel took it) is
+// used up. Block 0 clears the flag before it counts itself finished, so the
+// last block's decision for the next step lands after the clear.
+__device__ __forceinline__ void consume_decision(const Arena& a) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.glob->decided = 0u;
+}
+
 __device__ __forceinline__ bool rebuilding(const Arena& a, uint32_t b) {
     return a.ctrl[b].rebuild != 0u;
 }
@@ -143,12 +150,19 @@ __device__ __forceinline__ bool grid_pass(const Arena& a) {
 // reorder_every-th rebuild (counted before the increment, as the reference).
 // With `set`, the verdict (some box rebuilds) becomes the value of the graph
 // conditional `handle`.
+// A step kernel's last block takes the next step's decision itself
+// (`folded`) and leaves Global::decided set; the step that follows consumes
+// it (its step kernel clears the flag). A decide that finds such a decision
+// not yet consumed keeps it -- the displacements it came from were reset --
+// and only adds the boxes whose rebuild was forced since.
 __device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditionalHandle handle,
-                                             bool set) {
-    __shared__ int s_any;
+                                             bool set, bool folded = false) {
+    __shared__ int s_any, s_keep;
     Global* g = a.glob;
     if (threadIdx.x == 0) {
         s_any = 0;
+        s_keep = !folded && g->decided != 0u;
+        g->decided = folded ? 1u : 0u;
         g->work_front = 0u;
         g->work_back = 0u;
         g->next_build = 0u;
@@ -159,11 +173,18 @@ __device__ __forceinline__ void decide_block(const Arena& a, cudaGraphConditiona
         }
     }
     __syncthreads();
+    const bool keep = s_keep != 0;
     for (uint32_t b = threadIdx.x; b < a.nboxes; b += blockDim.x) {
         Control& c = a.ctrl[b];
         const Box& bx = a.boxes[b];
-        const float moved = __uint_as_float(c.max_disp);
-        c.max_disp = 0u;
+        if (keep && c.rebuild) {
+            // decided at the end of the last step
+            c.forced = 0u;
+            s_any = 1;
+            continue;
+        }
+        const float moved = keep ? 0.0f : __uint_as_float(c.max_disp);
+        if (!keep) c.max_disp = 0u;
         const bool rebuild = moved > bx.half_skin2 || c.built == 0u || c.forced != 0u;
         c.forced = 0u;
         c.rebuild = rebuild ? 1u : 0u;

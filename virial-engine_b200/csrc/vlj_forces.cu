@@ -462,6 +462,7 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
                                                              const __grid_constant__ CUtensorMap map,
                                                              cudaGraphConditionalHandle next) {
     count_kernel(a);
+    consume_decision(a);
     __shared__ __align__(128) Stage st;
     const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
     const bool valid = i < a.nslots;
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
         a.glob->blocks_done = 0u;
         if (HEAT) a.glob->heat_next += 1u;
     }
-    if (next) decide_block(a, next, true);
+    if (next) decide_block(a, next, true, true);
 }
 
 // ---- one step over cell tiles: the same step as step_kernel, with the
@@ -514,6 +515,7 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
 template <bool SHIFTED_FORCE, bool HEAT>
 __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphConditionalHandle next) {
     count_kernel(a);
+    consume_decision(a);
     extern __shared__ __align__(16) uint4 s_tile[];
     __shared__ uint32_t s_run[9][3];  // per tile row: first run's sorted start, its length, second run's start
     __shared__ uint32_t s_base[10];   // tile index of each row's first particle; [9]: the tile's size
@@ -681,7 +683,7 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
         a.glob->blocks_done = 0u;
         if (HEAT) a.glob->heat_next += 1u;
     }
-    if (next) decide_block(a, next, true);
+    if (next) decide_block(a, next, true, true);
 }
 
 // ---- measure (lennard_jones.wgsl:576-626) ----

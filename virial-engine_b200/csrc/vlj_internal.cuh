@@ -162,6 +162,8 @@ struct Global {
     uint32_t rb_boxes;           // boxes that rebuild this step (Arena::rb_box)
     uint32_t rb_slots;           // their particles, in all
     uint32_t heat_next;          // heat-current samples written to the series so far
+    uint32_t decided;            // a step kernel took the next step's decision, not yet consumed
+    uint32_t pad;
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).

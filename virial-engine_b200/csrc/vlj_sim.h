@@ -78,6 +78,13 @@ struct vlj_sim {
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph_chunk = nullptr;
     cudaGraphExec_t graph_one = nullptr;
+    // graph_one's template (kept for node updates) and its decide node: while
+    // the last step enqueued was graph_one's, whose step kernel took this
+    // step's decision and set graph_one's condition, the node is disabled
+    cudaGraph_t graph_one_tmpl = nullptr;
+    cudaGraphNode_t one_decide = nullptr;
+    bool one_decide_on = true;
+    bool one_ready = false;
     cudaGraphExec_t graph_one_heat = nullptr;  // one step that also takes the pending sample
     cudaGraphExec_t graph_lists = nullptr;  // decide -> IF(rebuild){rebuild chain}
     // per-launch timing of the step kernel (direct launches while on)
