@@ -16,8 +16,16 @@ The winner's settings become the defaults of VLJ_LIST_STREAM / VLJ_L1_CARVEOUT
     python virial-engine_b200/tune.py --kernel build [--cells 40] [--steps 30]
 
 times the list build's variants instead (candidates per round, staged
-candidates per warp, blocks per SM: VLJ_BUILD_* in csrc/vlj_build.cu) by the
-wall time of a forced rebuild.
+candidates per warp, blocks per SM, two home particles per test:
+VLJ_BUILD_* in csrc/vlj_build.cu) by the wall time of a forced rebuild.
+
+    python virial-engine_b200/tune.py --kernel tiles [--cells 40] [--steps 40]
+
+times the step kernel with cell tiles (VLJ_TILES=1) against the per-particle
+gathers: bricks per x-row 3, 4, 5, 6, 8 (the tile size and the threads per
+block follow from it; VLJ_TILE_COLS at run time) for the encoded-word tiles,
+f32 offsets from the brick centre (VLJ_TILE_F32) and the next row read ahead
+(VLJ_TILE_PIPE).
 """
 
 import argparse
@@ -33,7 +41,14 @@ OUT_DIR = os.path.join(HERE, "build", "tune")
 # tiles in flight)
 # list-build variants: candidates fetched per round, staged per warp, and the
 # blocks per SM the registers are sized for
-BUILD_CANDIDATES = {
+BUILD_# cell-tile variants: compile-time form x bricks per x-row (0: tiles off)
+TILE_CANDIDATES = {
+    "encoded": {},
+    "f32": {"VLJ_TILE_F32": 1},
+    "read_ahead": {"VLJ_TILE_PIPE": 1},
+}
+TILE_COLS = (0, 3, 4, 5, 6, 8)
+CANDIDATES = {
     "single_stage448_b6": {"VLJ_BUILD_PAIRS": 0},
     "single_stage512_b6": {"VLJ_BUILD_PAIRS": 0, "VLJ_BUILD_STAGE": 512},
     "pairs_stage448_b6": {},
@@ -41,6 +56,13 @@ BUILD_CANDIDATES = {
     "pairs_stage384_b7": {"VLJ_BUILD_PAIRS": 1, "VLJ_BUILD_STAGE": 384,
                           "VLJ_BUILD_BLOCKS_PER_SM": 7},
 }
+# cell-tile variants: compile-time form x bricks per x-row (0: tiles off)
+TILE_CANDIDATES = {
+    "encoded": {},
+    "f32": {"VLJ_TILE_F32": 1},
+    "read_ahead": {"VLJ_TILE_PIPE": 1},
+}
+TILE_COLS = (0, 3, 4, 5, 6, 8)
 CANDIDATES = {
     "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
     "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
@@ -52,8 +74,12 @@ CANDIDATES = {
 }
 
 
-def child(lib, cells, steps):
+def child(lib, cells, steps, cols=None):
     os.environ["VLJ_LIBRARY"] = lib
+    if cols is not None:
+        os.environ["VLJ_TILES"] = "1" if cols else "0"
+        if cols:
+            os.environ["VLJ_TILE_COLS"] = str(cols)
     sys.path.insert(0, HERE)
     import torch
     import virial_lj as vl
@@ -70,7 +96,8 @@ def child(lib, cells, steps):
             flush.fill_(1)
         sim.step(1)
     ms, n = sim.kernel_time()
-    print(json.dumps({"step_kernel_us": ms * 1e3 / n, "launches": n}))
+    print(json.dumps({"step_kernel_us": ms * 1e3 / n, "launches": n,
+                      "tiles": list(sim.tile_info())}))
 
 
 def build_child(lib, cells, rebuilds):
@@ -97,8 +124,10 @@ def main():
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--child", default=None)
-    ap.add_argument("--kernel", choices=["step", "build"], default="step",
-                    help="tune the force kernels' list reading (step) or the list build")
+    ap.add_argument("--kernel", choices=["step", "build", "tiles"], default="step",
+                    help="tune the force kernels' list reading (step), the list build, or "
+                         "the cell-tile step kernel against the gathers (tiles)")
+    ap.add_argument("--cols", type=int, default=None, help=argparse.SUPPRESS)
     ap.add_argument("--no-build", action="store_true",
                     help="time the variants already in build/tune (built elsewhere)")
     ap.add_argument("--build-only", action="store_true", help="build the variants, time nothing")
@@ -107,13 +136,13 @@ def main():
         if args.kernel == "build":
             build_child(args.child, args.cells, args.steps)
         else:
-            child(args.child, args.cells, args.steps)
+            child(args.child, args.cells, args.steps, args.cols)
         return
     sys.path.insert(0, HERE)
     import build
     os.makedirs(OUT_DIR, exist_ok=True)
     results = []
-    candidates = BUILD_CANDIDATES if args.kernel == "build" else CANDIDATES
+    candidates = {"build": BUILD_CANDIDATES, "tiles": TILE_CANDIDATES}.get(args.kernel, CANDIDATES)
     key = "rebuild_us" if args.kernel == "build" else "step_kernel_us"
     for name, defines in candidates.items():
         lib = os.path.join(OUT_DIR, f"libvirial_lj_{name}.so")
@@ -121,16 +150,21 @@ def main():
             build.build(defines=defines, out=lib, force=True)
         if args.build_only:
             continue
-        out = subprocess.run([sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
-                              "--steps", str(args.steps), "--kernel", args.kernel],
-                             capture_output=True, text=True)
-        if out.returncode != 0:
-            print(json.dumps({"variant": name, "error": out.stderr[-500:]}), flush=True)
-            continue
-        r = json.loads(out.stdout.strip().splitlines()[-1])
-        r.update(variant=name, defines=defines)
-        results.append(r)
-        print(json.dumps(r), flush=True)
+        for cols in (TILE_COLS if args.kernel == "tiles" else (None,)):
+            if args.kernel == "tiles" and cols == 0 and name != "encoded":
+                continue  # tiles off: the same kernel in every variant
+            cmd = [sys.executable, __file__, "--child", lib, "--cells", str(args.cells),
+                   "--steps", str(args.steps), "--kernel", args.kernel]
+            if cols is not None:
+                cmd += ["--cols", str(cols)]
+            out = subprocess.run(cmd, capture_output=True, text=True)
+            if out.returncode != 0:
+                print(json.dumps({"variant": name, "error": out.stderr[-500:]}), flush=True)
+                continue
+            r = json.loads(out.stdout.strip().splitlines()[-1])
+            r.update(variant=name if cols is None else f"{name}_cols{cols}", defines=defines)
+            results.append(r)
+            print(json.dumps(r), flush=True)
     if results:
         best = min(results, key=lambda r: r[key])
         print(json.dumps({"best": best}))
