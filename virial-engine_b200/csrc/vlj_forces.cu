@@ -150,9 +150,9 @@ __device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const u
         // integer differences times the box step are exact in f64): on a
         // lattice, where every pair at one distance rounds alike, the f32
         // components' three roundings would bias the virial coherently.
-        const double ex = exact_double((int32_t)(pj.x - own.x)) * (double)dec0;
-        const double ey = exact_double((int32_t)(pj.y - own.y)) * (double)dec1;
-        const double ez = exact_double((int32_t)(pj.z - own.z)) * (double)dec2;
+        const double ex = (double)(int32_t)(pj.x - own.x) * (double)dec0;
+        const double ey = (double)(int32_t)(pj.y - own.y) * (double)dec1;
+        const double ez = (double)(int32_t)(pj.z - own.z) * (double)dec2;
         float rf, u, t, e;
         lj_pair<SHIFTED_FORCE>((float)(ex * ex + ey * ey + ez * ez), bx, rf, u);
         two_sum(s.pe, 0.5f * u, t, e);

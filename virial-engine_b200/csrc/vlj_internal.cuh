@@ -289,13 +289,6 @@ __device__ __forceinline__ long long fixed_raw_f64(double x) {
     return __double2ll_rn(x * 4294967296.0);
 }
 
-// A 32-bit integer as an f64, exactly, on the FP64 adder rather than the
-// conversion unit: the double 2^52 + 2^31 + d has d + 2^31 in the low word of
-// its mantissa.
-__device__ __forceinline__ double exact_double(int32_t d) {
-    return __hiloint2double(0x43300000, (uint32_t)d ^ 0x80000000u) - 4503601774854144.0;
-}
-
 // ---- position encoding ----
 __device__ __forceinline__ uint32_t encode(double x, double enc) {
     return (uint32_t)(unsigned long long)__double2ll_rn(x * enc);
