@@ -1,9 +1,11 @@
 // Sampling kernels, sm_100a: profiles along z (Irving-Kirkwood) and the
-// microscopic heat current. Both walk each particle's Verlet list once with
-// the force kernels' arithmetic (so the canonical velocity v + a dt/2 they
-// need is the measurement's, bit for bit) and add 32.32 fixed-point sums
-// without a scale factor, as the reference does. Samples are taken every tens
-// of steps, so these are one thread per particle with plain list loads.
+// microscopic heat current. Both walk each particle's Verlet list with the
+// force kernels' pair arithmetic (the force factor, and the energy as the
+// heat current's fused pass takes it) and add 32.32 fixed-point sums without
+// a scale factor, as the reference does. The heat current walks each list in
+// one thread, in list order, so the canonical velocity v + a dt/2 it needs is
+// the measurement's bit for bit; the profile splits each list over several
+// threads.
 #include <cuda_runtime.h>
 
 #include "vlj_device.cuh"
@@ -50,6 +52,15 @@ __device__ __forceinline__ void walk_pairs(const Arena& a, const Box& bx, uint32
 // to one). After the slabs come three whole-box W_aa. The per-block sums
 // collect in shared memory when they fit, then flush with one atomic per
 // touched slot.
+//
+// kProfileLanes consecutive threads share a particle: each walks every
+// kProfileLanes-th row of its list (four entries a row) and spreads those
+// pairs; the force for the canonical velocity is their partial sums added
+// in a fixed order (shuffles), so it is the same on every run. Samples of
+// small boxes (the 16,000-atom slab) would otherwise give the GPU too few
+// threads to hide a list walk's latency.
+constexpr int kProfileLanes = 8;
+
 template <bool SHIFTED_FORCE>
 __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in_shared) {
     count_kernel(a);
@@ -65,20 +76,43 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in
     auto add = [&](uint32_t slot, long long raw) {
         if (raw) atomicAdd(acc + slot, (unsigned long long)raw);
     };
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.nslots) {
-        const float width = bx.bin_width;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / (uint32_t)kProfileLanes, sub = t % (uint32_t)kProfileLanes;
+    const bool valid = i < a.nslots;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    int32_t home = 0;
+    if (valid) {
+        const uint4* __restrict__ cur = a.cache[a.glob->phase];
+        const float width = bx.bin_width, inv_width = 1.0f / width;
         const int32_t nb = (int32_t)bins;
         const float z = (float)a.x[2 * (size_t)a.seg + i];
-        int32_t home = (int32_t)floorf(z / width);
+        home = (int32_t)floorf(z / width);
         home = home < 0 ? 0 : (home > nb - 1 ? nb - 1 : home);
         float pe = 0.0f, tot[3] = {0.0f, 0.0f, 0.0f};
-        float ax, ay, az;
-        walk_pairs<SHIFTED_FORCE>(a, bx, i, a.cache[a.glob->phase], ax, ay, az,
-            [&](float dx, float dy, float dz, float r2, float rf, float u) {
-                pe += 0.5f * u;
-                const float q = rf / r2;
-                const float w[3] = {0.5f * dx * dx * q, 0.5f * dy * dy * q, 0.5f * dz * dz * q};
+        const uint4 own = cur[i];
+        const uint32_t cnt = a.list_count[i];
+        const uint32_t rows = (cnt + 3u) / 4u;
+        const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;
+        for (uint32_t r = sub; r < rows; r += (uint32_t)kProfileLanes) {
+            const uint4 e = rowp[(size_t)r * a.seg];
+            const uint32_t js[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+            for (int q4 = 0; q4 < 4; q4++) {
+                const uint4 pj = cur[js[q4]];
+                const float dx = decode_diff(pj.x, own.x, bx.dec[0]);
+                const float dy = decode_diff(pj.y, own.y, bx.dec[1]);
+                const float dz = decode_diff(pj.z, own.z, bx.dec[2]);
+                const float r2 = sep_r2(dx, dy, dz);
+                // the last row's padding (the particle itself) and the
+                // entries past the cutoff drop out here
+                if (!(r2 < bx.rc2) || r2 == 0.0f) continue;
+                const float f = lj_force_over_r2<SHIFTED_FORCE>(r2, bx.force_shift);
+                ax = __fmaf_rn(-dx, f, ax);
+                ay = __fmaf_rn(-dy, f, ay);
+                az = __fmaf_rn(-dz, f, az);
+                pe += 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx);
+                // f = |F| / r, so r_a F_a = d_a^2 f
+                const float w[3] = {0.5f * dx * dx * f, 0.5f * dy * dy * f, 0.5f * dz * dz * f};
 #pragma unroll
                 for (int c = 0; c < 3; c++) tot[c] += w[c];
                 const float lo = z + fminf(dz, 0.0f);
@@ -87,39 +121,52 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in
                 if (length < 1e-6f * width) {
 #pragma unroll
                     for (int c = 0; c < 3; c++) add(home * kProfileSlots + 4 + c, fixed_raw_f32(w[c]));
-                    return;
+                    continue;
                 }
-                int32_t b = (int32_t)floorf(lo / width);
+                const float inv_length = 1.0f / length;
+                int32_t b = (int32_t)floorf(lo * inv_width);
                 float left = 1.0f;
                 for (;;) {
                     const bool last = (float)(b + 1) * width >= hi;
                     const float start = fmaxf(lo, (float)b * width);
                     const float end = fminf(hi, (float)(b + 1) * width);
-                    float share = last ? left : (end - start) / length;
+                    float share = last ? left : (end - start) * inv_length;
                     share = fmaxf(share, 0.0f);
                     left -= share;
-                    const int32_t slab = ((b % nb) + nb) % nb;
+                    // b lies within one box length of the home slab
+                    const int32_t slab = b < 0 ? b + nb : (b >= nb ? b - nb : b);
 #pragma unroll
                     for (int c = 0; c < 3; c++)
                         add((uint32_t)slab * kProfileSlots + 4 + c, fixed_raw_f32(w[c] * share));
                     if (last) break;
                     b += 1;
                 }
-            });
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) add(bins * kProfileSlots + c, fixed_raw_f32(tot[c]));
+        add((uint32_t)home * kProfileSlots + 7, fixed_raw_f32(pe));
+    }
+    // the particle's force: its lanes' partial sums, added pairwise
+#pragma unroll
+    for (int o = 1; o < kProfileLanes; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (valid && sub == 0u) {
         const float acc3[3] = {ax, ay, az};
         add((uint32_t)home * kProfileSlots, 1ll << 32);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const double v = canonical_velocity(a, bx, 0, i, c, acc3[c]);
             add((uint32_t)home * kProfileSlots + 1 + c, fixed_raw_f64(v * v));
-            add(bins * kProfileSlots + c, fixed_raw_f32(tot[c]));
         }
-        add((uint32_t)home * kProfileSlots + 7, fixed_raw_f32(pe));
     }
     if (in_shared) {
         __syncthreads();
-        for (uint32_t t = threadIdx.x; t < words; t += blockDim.x)
-            if (s_prof[t]) atomicAdd(&a.profile[t], s_prof[t]);
+        for (uint32_t t2 = threadIdx.x; t2 < words; t2 += blockDim.x)
+            if (s_prof[t2]) atomicAdd(&a.profile[t2], s_prof[t2]);
     }
 }
 
@@ -218,7 +265,7 @@ cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cu
     const size_t words = (size_t)bins * kProfileSlots + 3;
     const size_t bytes = words * sizeof(unsigned long long);
     const int in_shared = bytes <= 48 * 1024 ? 1 : 0;
-    const unsigned blocks = blocks_for(a.nslots, kSampleThreads);
+    const unsigned blocks = blocks_for((uint64_t)a.nslots * kProfileLanes, kSampleThreads);
     const size_t smem = in_shared ? bytes : 0;
     if (shifted_force)
         profile_kernel<true><<<blocks, kSampleThreads, smem, s>>>(a, in_shared);
