@@ -64,34 +64,21 @@ constexpr int kProfileLanes = 8;
 // IN_SHARED: the block's sums in shared memory (the address space known to
 // the compiler, so the atomics are shared-memory ones), else straight into
 // the profile in global memory.
-// In shared memory each 64-bit sum is two 32-bit words added with native
-// 32-bit atomics, the low word's carry (read from the atomic's old value)
-// going into the high word -- the reference's scheme (fixed.wgsl:20-65):
-// exact and order-independent, where a 64-bit shared atomic would be a
-// compare-and-swap loop that contended slabs keep retrying.
-__device__ __forceinline__ void add_fixed_shared(uint32_t* words2, uint32_t slot, long long raw) {
-    const unsigned long long u = (unsigned long long)raw;
-    const uint32_t lo = (uint32_t)u, hi = (uint32_t)(u >> 32);
-    const uint32_t old = atomicAdd(&words2[2 * slot], lo);
-    const uint32_t carry = old + lo < old ? 1u : 0u;
-    if (hi + carry) atomicAdd(&words2[2 * slot + 1], hi + carry);
-}
-
 template <bool SHIFTED_FORCE, bool IN_SHARED>
 __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a) {
     count_kernel(a);
-    extern __shared__ uint32_t s_prof[];  // (low, high) word pairs
+    extern __shared__ unsigned long long s_prof[];
     const Box& bx = a.boxes[0];
     const uint32_t bins = bx.profile_bins;
     const uint32_t words = bins * kProfileSlots + 3u;
     if (IN_SHARED) {
-        for (uint32_t t = threadIdx.x; t < 2 * words; t += blockDim.x) s_prof[t] = 0u;
+        for (uint32_t t = threadIdx.x; t < words; t += blockDim.x) s_prof[t] = 0ull;
         __syncthreads();
     }
     auto add = [&](uint32_t slot, long long raw) {
         if (!raw) return;
         if (IN_SHARED)
-            add_fixed_shared(s_prof, slot, raw);
+            atomicAdd(&s_prof[slot], (unsigned long long)raw);
         else
             atomicAdd(&a.profile[slot], (unsigned long long)raw);
     };
@@ -184,11 +171,8 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a) {
     }
     if (IN_SHARED) {
         __syncthreads();
-        for (uint32_t t2 = threadIdx.x; t2 < words; t2 += blockDim.x) {
-            const unsigned long long v =
-                ((unsigned long long)s_prof[2 * t2 + 1] << 32) | s_prof[2 * t2];
-            if (v) atomicAdd(&a.profile[t2], v);
-        }
+        for (uint32_t t2 = threadIdx.x; t2 < words; t2 += blockDim.x)
+            if (s_prof[t2]) atomicAdd(&a.profile[t2], s_prof[t2]);
     }
 }
 
