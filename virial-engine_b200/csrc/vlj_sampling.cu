@@ -61,26 +61,20 @@ __device__ __forceinline__ void walk_pairs(const Arena& a, const Box& bx, uint32
 // threads to hide a list walk's latency.
 constexpr int kProfileLanes = 8;
 
-// IN_SHARED: the block's sums in shared memory (the address space known to
-// the compiler, so the atomics are shared-memory ones), else straight into
-// the profile in global memory.
-template <bool SHIFTED_FORCE, bool IN_SHARED>
-__global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a) {
+template <bool SHIFTED_FORCE>
+__global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a, int in_shared) {
     count_kernel(a);
     extern __shared__ unsigned long long s_prof[];
     const Box& bx = a.boxes[0];
     const uint32_t bins = bx.profile_bins;
     const uint32_t words = bins * kProfileSlots + 3u;
-    if (IN_SHARED) {
+    if (in_shared) {
         for (uint32_t t = threadIdx.x; t < words; t += blockDim.x) s_prof[t] = 0ull;
         __syncthreads();
     }
+    unsigned long long* acc = in_shared ? s_prof : a.profile;
     auto add = [&](uint32_t slot, long long raw) {
-        if (!raw) return;
-        if (IN_SHARED)
-            atomicAdd(&s_prof[slot], (unsigned long long)raw);
-        else
-            atomicAdd(&a.profile[slot], (unsigned long long)raw);
+        if (raw) atomicAdd(acc + slot, (unsigned long long)raw);
     };
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t i = t / (uint32_t)kProfileLanes, sub = t % (uint32_t)kProfileLanes;
@@ -169,7 +163,7 @@ __global__ void __launch_bounds__(kSampleThreads) profile_kernel(Arena a) {
             add((uint32_t)home * kProfileSlots + 1 + c, fixed_raw_f64(v * v));
         }
     }
-    if (IN_SHARED) {
+    if (in_shared) {
         __syncthreads();
         for (uint32_t t2 = threadIdx.x; t2 < words; t2 += blockDim.x)
             if (s_prof[t2]) atomicAdd(&a.profile[t2], s_prof[t2]);
@@ -273,13 +267,10 @@ cudaError_t launch_profile(const Arena& a, uint32_t bins, bool shifted_force, cu
     const int in_shared = bytes <= 48 * 1024 ? 1 : 0;
     const unsigned blocks = blocks_for((uint64_t)a.nslots * kProfileLanes, kSampleThreads);
     const size_t smem = in_shared ? bytes : 0;
-    if (shifted_force) {
-        if (in_shared) profile_kernel<true, true><<<blocks, kSampleThreads, smem, s>>>(a);
-        else profile_kernel<true, false><<<blocks, kSampleThreads, 0, s>>>(a);
-    } else {
-        if (in_shared) profile_kernel<false, true><<<blocks, kSampleThreads, smem, s>>>(a);
-        else profile_kernel<false, false><<<blocks, kSampleThreads, 0, s>>>(a);
-    }
+    if (shifted_force)
+        profile_kernel<true><<<blocks, kSampleThreads, smem, s>>>(a, in_shared);
+    else
+        profile_kernel<false><<<blocks, kSampleThreads, smem, s>>>(a, in_shared);
     return after_launch();
 }
 
