@@ -303,6 +303,30 @@ VLJ_API vlj_status vlj_bin_noalloc(const double *pos, size_t count, const double
                                    const uint32_t cells[3], uint32_t *sorted,
                                    uint32_t *cell_start, uint32_t *cell_of, void *stream);
 
+/* ---- granular contacts through the cell grid ----
+ * The reference's granular solver includes the same grid (granular.rs:
+ * 327-328 appends grid.wgsl): grains binned into cells at least one diameter
+ * wide, each cell sorted by grain index, and every grain's contacts found in
+ * the 27 cells around its own -- not periodic: cells past a wall are skipped
+ * -- in the order dz, dy, dx = -1..1, each in its sorted order
+ * (granular.wgsl:204-263). vlj_grain_cells gives the reference's cells per
+ * axis, clamp(floor(box_size / (2 max_radius)), 1, 64) (granular.rs:
+ * 179-181). vlj_grain_contacts bins `count` grains (pos: count x 3 doubles,
+ * radius: count doubles; device memory) into cells^3 cubic cells of side
+ * box_size / cells and writes, for grain i, its overlapping partners in that
+ * order to partners[i * capacity ..] (the first `capacity` of them) and their
+ * number to counts[i]; the reference's test is double-float positions, f32
+ * radii, reach - sqrt(dot(d, d)) > 0. It also leaves the grid: sorted
+ * (count), cell_start (cells^3 + 1), cell_of (count). Every buffer is the
+ * caller's, device memory, including `scratch` (cells^3 + 1 words); nothing
+ * is allocated. Enqueued on `stream`. */
+VLJ_API vlj_status vlj_grain_cells(double box_size, double max_radius, uint32_t *cells);
+VLJ_API vlj_status vlj_grain_contacts(const double *pos, const double *radius, size_t count,
+                                      double box_size, uint32_t cells, uint32_t capacity,
+                                      uint32_t *scratch, uint32_t *sorted, uint32_t *cell_start,
+                                      uint32_t *cell_of, uint32_t *partners, uint32_t *counts,
+                                      void *stream);
+
 /* ---- inspection for tests (no reference counterpart) ----
  * Reads the grid and lists of the last rebuild: slot of each position in
  * cell order (`sorted`, n), cell starts (total_cells + 1), cell of each slot

@@ -355,3 +355,76 @@ class DoubleFloatMD:
 
     def __del__(self):
         self.close()
+
+
+# ---- granular contacts through the cell grid (test oracle) ----
+
+def grain_block(lo, hi, radius, spread, seed):
+    """Grains on a jittered cubic lattice filling [lo, hi] (granular.rs:634-665):
+    spacing 2 r (1 + spread) 1.02, xorshift64 seeded with seed | 1, positions
+    jittered by +-1 % of r, radii r (1 + spread (2 u - 1)). Returns (pos, radius)."""
+    spacing = 2.0 * radius * (1.0 + spread) * 1.02
+    counts = [max(int(np.floor((hi[k] - lo[k]) / spacing)), 1) for k in range(3)]
+    mask = (1 << 64) - 1
+    s = (seed | 1) & mask
+
+    def random():
+        nonlocal s
+        s ^= (s << 13) & mask
+        s ^= s >> 7
+        s ^= (s << 17) & mask
+        return (s >> 11) / float(1 << 53)
+
+    pos, rad = [], []
+    for z in range(counts[2]):
+        for y in range(counts[1]):
+            for x in range(counts[0]):
+                jit = [(random() - 0.5) * 0.02 * radius for _ in range(3)]
+                pos.append([lo[0] + (x + 0.5) * spacing + jit[0],
+                            lo[1] + (y + 0.5) * spacing + jit[1],
+                            lo[2] + (z + 0.5) * spacing + jit[2]])
+                rad.append(radius * (1.0 + spread * (2.0 * random() - 1.0)))
+    return np.array(pos), np.array(rad)
+
+
+def grain_contacts(pos, radius, box_size, cells, capacity):
+    """The granular solver's contact search (granular.wgsl:204-263) on its
+    grid (grid.wgsl:11-148; cell side f32(box / cells), granular.rs:182):
+    for each grain, the overlapping grains of the 27 cells around its own
+    (skipping cells past the walls) in the order dz, dy, dx, each cell in
+    grain order; double-float positions, f32 radii, IEEE f32 operations as
+    written. Returns (partners n x capacity, -1 where empty; counts)."""
+    f32 = np.float32
+    n = len(pos)
+    hi = pos.astype(f32)
+    lo = (pos - hi.astype(np.float64)).astype(f32)
+    rad = radius.astype(f32)
+    size = f32(box_size / cells)
+    c = np.floor(hi / size).astype(np.int64)
+    c = np.clip(c, 0, cells - 1)
+    cell = (c[:, 2] * cells + c[:, 1]) * cells + c[:, 0]
+    order = np.argsort(cell, kind="stable")
+    start = np.searchsorted(cell[order], np.arange(cells ** 3 + 1))
+    partners = np.full((n, capacity), -1, np.int64)
+    counts = np.zeros(n, np.int64)
+    for i in range(n):
+        cand = []
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    q = c[i] + np.array([dx, dy, dz])
+                    if (q < 0).any() or (q >= cells).any():
+                        continue
+                    k = (q[2] * cells + q[1]) * cells + q[0]
+                    cand.extend(order[start[k]:start[k + 1]])
+        cand = np.array([j for j in cand if j != i], np.int64)
+        if len(cand) == 0:
+            continue
+        d = (hi[i] - hi[cand]) + (lo[i] - lo[cand])
+        dist2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        reach = rad[i] + rad[cand]
+        dist = np.sqrt(dist2)
+        hit = cand[((reach - dist) > f32(0)) & (dist2 > f32(0))]
+        counts[i] = len(hit)
+        partners[i, :min(len(hit), capacity)] = hit[:capacity]
+    return partners, counts

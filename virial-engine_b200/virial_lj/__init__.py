@@ -29,7 +29,7 @@ __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
     "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
-    "replica_cost", "shard_replicas", "tune_batch_skin",
+    "replica_cost", "shard_replicas", "tune_batch_skin", "grain_cells", "grain_contacts",
 ]
 
 
@@ -77,6 +77,41 @@ def philox(ctr, key):
     _check(_lib.vlj_debug_philox(_ffi.ptr(ctr), _ffi.ptr(key), len(ctr), _ffi.ptr(out),
                                  _ffi.ptr(noise)))
     return out, noise
+
+
+def grain_cells(box_size, max_radius):
+    """Cells per axis of the granular solver's grid (granular.rs:179-181)."""
+    c = C.c_uint32()
+    _check(_lib.vlj_grain_cells(float(box_size), float(max_radius), C.byref(c)))
+    return c.value
+
+
+def grain_contacts(pos, radius, box_size, capacity=16, cells=None, stream=None):
+    """Overlapping partners of every grain through the cell grid, in the
+    reference's order (granular.wgsl:204-263). `pos` (n x 3) and `radius` (n)
+    are torch tensors of float64 on the device (the entry point works on
+    device memory and allocates nothing; the buffers here are torch's).
+    Returns (partners n x capacity, counts n, sorted, cell_start, cell_of)
+    as torch int32 tensors on the device."""
+    import torch
+    n = pos.shape[0]
+    if cells is None:
+        cells = grain_cells(box_size, float(radius.max()))
+    dev = pos.device
+    i32 = dict(dtype=torch.int32, device=dev)
+    total = cells ** 3
+    scratch = torch.zeros(total + 1, **i32)
+    sorted_, cell_start = torch.zeros(n, **i32), torch.zeros(total + 1, **i32)
+    cell_of, counts = torch.zeros(n, **i32), torch.zeros(n, **i32)
+    partners = torch.full((n, max(capacity, 1)), -1, **i32)
+    pos = pos.contiguous()
+    radius = radius.contiguous()
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(_lib.vlj_grain_contacts(pos.data_ptr(), radius.data_ptr(), n, float(box_size), cells,
+                                   capacity, scratch.data_ptr(), sorted_.data_ptr(),
+                                   cell_start.data_ptr(), cell_of.data_ptr(), partners.data_ptr(),
+                                   counts.data_ptr(), s))
+    return partners, counts, sorted_, cell_start, cell_of
 
 
 def launches():

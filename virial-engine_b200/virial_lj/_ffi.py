@@ -121,6 +121,9 @@ SIGNATURES = {
     "vlj_debug_kernel_time": [_vp, _P(C.c_double), _P(C.c_uint64)],
     "vlj_debug_fp32_peak": [_P(C.c_double)],
     "vlj_debug_philox": [_vp, _vp, C.c_size_t, _vp, _vp],
+    "vlj_grain_cells": [C.c_double, C.c_double, _P(C.c_uint32)],
+    "vlj_grain_contacts": [_vp, _vp, C.c_size_t, C.c_double, C.c_uint32, C.c_uint32, _vp, _vp,
+                           _vp, _vp, _vp, _vp, _vp],
     "vlj_debug_set_tiles": [_vp, C.c_int],
     "vlj_debug_tile_info": [_vp, _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32)],
     "vlj_debug_read_tile_lists": [_vp, _vp],
