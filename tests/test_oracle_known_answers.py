@@ -184,3 +184,19 @@ def test_double_float_path_in_the_liquid(O, shifted_force):
     pe64, w64 = O.all_pairs(np.mod(p, box), box, 2.5, shifted_force)
     assert abs((pe - pe64) / pe64) < 1e-5 and abs((w - w64.sum()) / w64.sum()) < 1e-5
     assert abs(ke - 0.5 * np.sum(v * v)) < 1e-9 * ke
+
+
+def test_grain_oracle_block_and_symmetry(O):
+    # granular.rs:634-665: floor((hi - lo) / spacing) grains per axis, radii
+    # within r (1 +- spread), none overlapping at spacing 2 r (1 + spread) 1.02
+    pos, radius = O.grain_block([0.004, 0.004, 0.004], [0.03, 0.03, 0.02], 0.0015, 0.1, 7)
+    spacing = 2 * 0.0015 * 1.1 * 1.02
+    assert len(pos) == int(0.026 // spacing) ** 2 * int(0.016 // spacing)
+    assert radius.min() >= 0.0015 * 0.9 and radius.max() <= 0.0015 * 1.1
+    _, counts = O.grain_contacts(pos, radius, 0.05, 16, 16)
+    assert counts.max() == 0
+    # grown radii: the contact test is symmetric, so the partner relation is
+    partners, counts = O.grain_contacts(pos, radius * 1.12, 0.05, 16, 16)
+    assert counts.sum() > 0
+    pairs = {(i, int(j)) for i in range(len(pos)) for j in partners[i, :counts[i]]}
+    assert all((j, i) in pairs for i, j in pairs)
