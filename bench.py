@@ -53,7 +53,7 @@ ALGO_BYTES = 96          # f64 x and v read + written per particle-step
 
 BATCH = dict(replicas=512, seed=2024, sizes=(500, 20000), densities=(0.01, 0.90),
              temperatures=(0.7, 2.0), friction=1.0, dt=0.004, cutoff=2.5, skin=0.3,
-             skins=(0.3, 0.4, 0.5, 0.6, 0.8))
+             skins=(0.3, 0.4, 0.5, 0.6, 0.8), threads=(64, 128, 256))
 PLAIN_SAMPLE_EVERY = 16  # plain-path comparison: every 16th replica as its own simulation
 PLAIN_SAMPLE_STEPS = 50
 
@@ -252,11 +252,13 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
     reps = vl.uneven_replicas(BATCH["replicas"], BATCH["seed"] + 7919 * rank, BATCH["sizes"],
                               BATCH["densities"], BATCH["temperatures"], BATCH["friction"])
     total = sum(len(r.particles) for r in reps)
-    # the neighbour skin for this set, chosen by the autotuner on this GPU
-    skin, skin_times = vl.tune_batch_skin(reps, BATCH["skins"], cutoff=BATCH["cutoff"],
-                                          dt=BATCH["dt"], stream=stream)
+    # the neighbour skin and the step kernel's block size for this set, chosen
+    # by the autotuner on this GPU
+    skin, threads, tuned = vl.tune_batch(reps, BATCH["skins"], BATCH["threads"],
+                                         cutoff=BATCH["cutoff"], dt=BATCH["dt"], stream=stream)
     b = vl.Batch(reps, cutoff=BATCH["cutoff"], skin=skin, dt=BATCH["dt"],
                  stream=stream.cuda_stream)
+    b.set_step_threads(threads)
     b.step(max(args.warmup, 3))
     stream.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -322,8 +324,9 @@ def run_batched(args, world, rank, stream, flush_l2, hbm_peak, fp32_peak):
         "config": {"sizes": "N log-uniform in [500, 20000]", "densities": "uniform in [0.01, 0.90]",
                    "temperatures": "uniform in [0.7, 2.0], Langevin gamma=1.0",
                    "cutoff": BATCH["cutoff"], "cutoff_style": "truncated-shifted",
-                   "skin": skin, "skin_tuned_ms_per_step": {str(k): v * 1e3 for k, v in
-                                                             skin_times.items()},
+                   "skin": skin, "step_threads": threads,
+                   "tuned_ms_per_step": {f"skin {k[0]} threads {k[1]}": v * 1e3
+                                         for k, v in tuned.items()},
                    "plain_skin": BATCH["skin"], "dt": BATCH["dt"],
                    "seed": BATCH["seed"] + 7919 * rank,
                    "l2": "flushed between timed steps (256 MiB write on the stream)"},

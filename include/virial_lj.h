@@ -386,6 +386,10 @@ VLJ_API vlj_status vlj_debug_fp32_peak(double *tflops);
  * entries: entry k of sorted position p at [(k / 8) * segment * 8 + p * 8 +
  * k % 8]). */
 VLJ_API vlj_status vlj_debug_set_tiles(vlj_sim *sim, int on);
+/* Particles per block of the step kernel: 64, 128 (the default) or 256 (a
+ * tuning knob: virial_lj.tune_batch times it per replica set; the same
+ * trajectory to the bit). */
+VLJ_API vlj_status vlj_debug_set_step_threads(vlj_sim *sim, uint32_t threads);
 VLJ_API vlj_status vlj_debug_tile_info(vlj_sim *sim, uint32_t *brick_cols, uint32_t *bricks,
                                        uint32_t *tile_cap, uint32_t *threads);
 VLJ_API vlj_status vlj_debug_read_tile_lists(vlj_sim *sim, uint16_t *out);

@@ -132,3 +132,29 @@ def test_batch_errors(gpu):
         gpu.Batch([gpu.Replica(q, [9.0] * 3, gpu.NoseHoover(1.0, 0.5))])
     with pytest.raises(gpu.VljError, match="INVALID_ARG"):
         gpu.Batch([])
+
+
+def test_step_block_size_keeps_the_trajectory(gpu):
+    # the tuner's block-size knob changes how particles are grouped, not what
+    # they compute: the same replicas step to the same bits with 64, 128 and
+    # 256 particles per block (and a single box the same)
+    reps = gpu.uneven_replicas(12, 77, (500, 4000), (0.05, 0.85), (0.8, 1.6), 1.0)
+    out = []
+    for threads in (64, 128, 256):
+        b = gpu.Batch(reps, cutoff=2.5, skin=0.3, dt=0.004)
+        b.set_step_threads(threads)
+        b.run(60)
+        ms = b.measure()
+        out.append(([b.read_particles(r).tobytes() for r in range(len(reps))],
+                     [(m.potential, m.virial, m.list_rebuilds) for m in ms]))
+        b.close()
+    assert out[0] == out[1] == out[2]
+    p, L = gpu.lattice_fcc(8, 0.8442, 1.0, 3)
+    st = gpu.Settings([L] * 3, dt=0.005, shifted_force=True, thermostat=gpu.Langevin(1.0, 1.0, 2))
+    runs = []
+    for threads in (64, 256):
+        sim = gpu.LennardJones(p, st)
+        sim.set_step_threads(threads)
+        sim.run(50)
+        runs.append(sim.read_particles().tobytes())
+    assert runs[0] == runs[1]

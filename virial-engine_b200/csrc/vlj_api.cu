@@ -811,6 +811,17 @@ vlj_status vlj_debug_set_tiles(vlj_sim* s, int on) {
     return VLJ_OK;
 }
 
+vlj_status vlj_debug_set_step_threads(vlj_sim* s, uint32_t threads) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (threads != 64 && threads != 128 && threads != 256)
+        return fail(VLJ_INVALID_ARG, "step threads must be 64, 128 or 256");
+    if (threads == s->arena.step_threads) return VLJ_OK;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    sim_drop_step_graphs(s);
+    s->arena.step_threads = threads;
+    return VLJ_OK;
+}
+
 vlj_status vlj_debug_tile_info(vlj_sim* s, uint32_t* brick_cols, uint32_t* bricks,
                                uint32_t* tile_cap, uint32_t* threads) {
     if (!s || !brick_cols || !bricks || !tile_cap || !threads)
@@ -1009,6 +1020,7 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     a.nboxes = (uint32_t)boxes.size();
     a.nslots = n;
     a.seg = seg;
+    a.step_threads = kForceThreads;
     a.ncells = (uint32_t)cells;
     Box* d_box = nullptr;
     TRY(dalloc(s, &d_box, boxes.size()));

@@ -457,14 +457,17 @@ __global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
 // The new position goes to the other cache copy (neighbours still read this
 // step's), and the largest squared displacement since the last list build
 // feeds the next step's rebuild decision.
-template <bool SHIFTED_FORCE, bool HEAT>
-__global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Arena a,
+// THREADS particles per block (Arena::step_threads, tuned per replica set
+// by virial_lj.tune_batch; the TMA tile ring needs kForceThreads).
+template <bool SHIFTED_FORCE, bool HEAT, int THREADS>
+__global__ void __launch_bounds__(THREADS, kStepMinBlocks) step_kernel(Arena a,
                                                              const __grid_constant__ CUtensorMap map,
                                                              cudaGraphConditionalHandle next) {
+    static_assert(VLJ_LIST_STREAM || THREADS == kForceThreads, "TMA tiles need kForceThreads");
     count_kernel(a);
     consume_decision(a);
     __shared__ __align__(128) Stage st;
-    const uint32_t i = blockIdx.x * kForceThreads + threadIdx.x;
+    const uint32_t i = blockIdx.x * THREADS + threadIdx.x;
     const bool valid = i < a.nslots;
     const uint32_t phase = a.glob->phase;
     const uint32_t b = valid ? box_of_slot(a, i) : 0u;
@@ -479,7 +482,7 @@ __global__ void __launch_bounds__(kForceThreads, kStepMinBlocks) step_kernel(Are
     }
     float disp2 = 0.0f;
     if (valid) disp2 = advance_slot(a, bx, i, phase, s);
-    block_max_per_box(a, valid, b, blockIdx.x * kForceThreads, disp2);
+    block_max_per_box(a, valid, b, blockIdx.x * THREADS, disp2);
     if (i == 0) a.glob->pending = 1u;
     if (!next && !HEAT) return;
     // the last block to finish takes the next step's rebuild decision and
@@ -1038,10 +1041,6 @@ static void prefer_l1_once() {
     static bool done = false;
     if (done) return;
     done = true;
-    prefer_l1(step_kernel<true, false>);
-    prefer_l1(step_kernel<false, false>);
-    prefer_l1(step_kernel<true, true>);
-    prefer_l1(step_kernel<false, true>);
     prefer_l1(measure_kernel<true>);
     prefer_l1(measure_kernel<false>);
     prefer_l1(prime_kernel<true>);
@@ -1063,6 +1062,28 @@ cudaError_t launch_prime(const Arena& a, const CUtensorMap& map, bool shifted_fo
         prime_kernel<true><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
     else
         prime_kernel<false><<<particle_blocks(a), kForceThreads, 0, s>>>(a, map);
+    return after_launch();
+}
+
+template <int THREADS>
+static cudaError_t launch_step_kernel(const Arena& a, const CUtensorMap& map, bool shifted_force,
+                                      cudaStream_t s, cudaGraphConditionalHandle next, bool heat) {
+    static bool carved = false;
+    if (!carved) {
+        carved = true;
+        prefer_l1(step_kernel<true, false, THREADS>);
+        prefer_l1(step_kernel<false, false, THREADS>);
+        prefer_l1(step_kernel<true, true, THREADS>);
+        prefer_l1(step_kernel<false, true, THREADS>);
+    }
+    const unsigned blocks = blocks_for(a.nslots, THREADS);
+    if (shifted_force) {
+        if (heat) step_kernel<true, true, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+        else step_kernel<true, false, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+    } else {
+        if (heat) step_kernel<false, true, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+        else step_kernel<false, false, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+    }
     return after_launch();
 }
 
@@ -1093,15 +1114,11 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_for
         return heat ? launch_tile_step<false, true>(a, s, next)
                     : launch_tile_step<false, false>(a, s, next);
     }
-    const unsigned blocks = particle_blocks(a);
-    if (shifted_force) {
-        if (heat) step_kernel<true, true><<<blocks, kForceThreads, 0, s>>>(a, map, next);
-        else step_kernel<true, false><<<blocks, kForceThreads, 0, s>>>(a, map, next);
-    } else {
-        if (heat) step_kernel<false, true><<<blocks, kForceThreads, 0, s>>>(a, map, next);
-        else step_kernel<false, false><<<blocks, kForceThreads, 0, s>>>(a, map, next);
+    switch (VLJ_LIST_STREAM ? a.step_threads : (uint32_t)kForceThreads) {
+        case 64: return launch_step_kernel<64>(a, map, shifted_force, s, next, heat);
+        case 256: return launch_step_kernel<256>(a, map, shifted_force, s, next, heat);
+        default: return launch_step_kernel<kForceThreads>(a, map, shifted_force, s, next, heat);
     }
-    return after_launch();
 }
 
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_force,

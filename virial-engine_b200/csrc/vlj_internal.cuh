@@ -247,6 +247,7 @@ struct Arena {
     uint32_t bricks;     // bricks in all boxes: the tile step kernel's grid
     uint32_t tile_cap;   // tile entries (16 B each) a block stages in shared memory
     uint32_t tile_threads;  // threads of a tile step block
+    uint32_t step_threads;  // particles per block of the step kernel: 64, 128 or 256
     // per force block (kForceThreads slots), for the TMA tile ring only: rows
     // (four entries each) of the longest list in it, so a block stages only
     // the rows its particles use. Reset at each rebuild of

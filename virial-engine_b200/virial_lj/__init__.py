@@ -29,7 +29,8 @@ __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
     "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
-    "replica_cost", "shard_replicas", "tune_batch_skin", "grain_cells", "grain_contacts",
+    "replica_cost", "shard_replicas", "tune_batch_skin", "tune_batch", "grain_cells",
+    "grain_contacts",
 ]
 
 
@@ -508,6 +509,10 @@ class LennardJones:
     def set_graphs(self, on):
         _check(_lib.vlj_debug_set_graphs(self._h, int(bool(on))))
 
+    def set_step_threads(self, threads):
+        """Particles per block of the step kernel (64, 128 or 256)."""
+        _check(_lib.vlj_debug_set_step_threads(self._h, int(threads)))
+
     def set_tiles(self, on):
         """Cell tiles in the step kernel on or off (same trajectory either way)."""
         _check(_lib.vlj_debug_set_tiles(self._h, int(bool(on))))
@@ -630,6 +635,10 @@ class Batch:
         _check(_lib.vlj_debug_batch_sim(self._h, C.byref(h)))
         return h
 
+    def set_step_threads(self, threads):
+        """Particles per block of the step kernel (64, 128 or 256)."""
+        _check(_lib.vlj_debug_set_step_threads(self._sim(), int(threads)))
+
     def set_graphs(self, on):
         _check(_lib.vlj_debug_set_graphs(self._sim(), int(bool(on))))
 
@@ -733,6 +742,41 @@ def shard_replicas(replicas, world_size, cutoff=2.5, skin=0.3):
         shards[rank].append(i)
         load[rank] += costs[i]
     return [sorted(s) for s in shards]
+
+
+def tune_batch(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), threads=(64, 128, 256), cutoff=2.5,
+               dt=0.005, shifted_force=False, steps=60, warmup=20, stream=None):
+    """The neighbour skin and the step kernel's particles per block that step
+    this replica set fastest on this GPU.
+
+    The skin trades list length against rebuild frequency (tune_batch_skin);
+    the block size trades the step kernel's tail (blocks that straddle two
+    replicas, or hold a dense replica's long lists) against its scheduling
+    granularity. Every (skin, threads) pair runs `warmup` then `steps` steps
+    of the actual set, timed with CUDA events on `stream` (a torch stream);
+    the trajectory does not depend on the block size and only the list length
+    on the skin. Returns (skin, threads, {(skin, threads): seconds per step}).
+    """
+    import torch
+
+    s = stream or torch.cuda.current_stream()
+    times = {}
+    for skin in skins:
+        b = Batch(replicas, cutoff=cutoff, skin=skin, dt=dt, shifted_force=shifted_force,
+                  stream=s.cuda_stream)
+        b.step(warmup)
+        for t in threads:
+            b.set_step_threads(t)
+            b.step(3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.step(steps)
+            e1.record(s)
+            s.synchronize()
+            times[(skin, t)] = e0.elapsed_time(e1) / 1e3 / steps
+        b.close()
+    skin, t = min(times, key=times.get)
+    return skin, t, times
 
 
 def tune_batch_skin(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), cutoff=2.5, dt=0.005,

@@ -125,6 +125,7 @@ SIGNATURES = {
     "vlj_grain_contacts": [_vp, _vp, C.c_size_t, C.c_double, C.c_uint32, C.c_uint32, _vp, _vp,
                            _vp, _vp, _vp, _vp, _vp],
     "vlj_debug_set_tiles": [_vp, C.c_int],
+    "vlj_debug_set_step_threads": [_vp, C.c_uint32],
     "vlj_debug_tile_info": [_vp, _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32)],
     "vlj_debug_read_tile_lists": [_vp, _vp],
 }
