@@ -457,6 +457,19 @@ __global__ void __launch_bounds__(kForceThreads) prime_kernel(Arena a,
 // The new position goes to the other cache copy (neighbours still read this
 // step's), and the largest squared displacement since the last list build
 // feeds the next step's rebuild decision.
+// The block's run of particles when the blocks that share an SM in the
+// first wave take neighbouring runs (VLJ_STEP_REMAP): the hardware hands out
+// blocks g, g + sms, g + 2 sms, ... to one SM in that wave, so within each
+// group of sms x per_sm blocks the order is transposed; blocks past the last
+// whole group keep their own run. A bijection on [0, n).
+__device__ __forceinline__ uint32_t resident_neighbours(uint32_t b, uint32_t n, uint32_t sms,
+                                                       uint32_t per_sm) {
+    const uint32_t w = sms * per_sm;
+    if (w == 0u || b >= n / w * w) return b;
+    const uint32_t t = b % w;
+    return b - t + (t % sms) * per_sm + t / sms;
+}
+
 // THREADS particles per block (Arena::step_threads, tuned per replica set
 // by virial_lj.tune_batch; the TMA tile ring needs kForceThreads).
 template <bool SHIFTED_FORCE, bool HEAT, int THREADS>
@@ -467,7 +480,12 @@ __global__ void __launch_bounds__(THREADS, kStepMinBlocks) step_kernel(Arena a,
     count_kernel(a);
     consume_decision(a);
     __shared__ __align__(128) Stage st;
-    const uint32_t i = blockIdx.x * THREADS + threadIdx.x;
+#if VLJ_STEP_REMAP
+    const uint32_t vb = resident_neighbours(blockIdx.x, gridDim.x, a.remap_sms, a.remap_per_sm);
+#else
+    const uint32_t vb = blockIdx.x;
+#endif
+    const uint32_t i = vb * THREADS + threadIdx.x;
     const bool valid = i < a.nslots;
     const uint32_t phase = a.glob->phase;
     const uint32_t b = valid ? box_of_slot(a, i) : 0u;
@@ -482,7 +500,7 @@ __global__ void __launch_bounds__(THREADS, kStepMinBlocks) step_kernel(Arena a,
     }
     float disp2 = 0.0f;
     if (valid) disp2 = advance_slot(a, bx, i, phase, s);
-    block_max_per_box(a, valid, b, blockIdx.x * THREADS, disp2);
+    block_max_per_box(a, valid, b, vb * THREADS, disp2);
     if (i == 0) a.glob->pending = 1u;
     if (!next && !HEAT) return;
     // the last block to finish takes the next step's rebuild decision and
@@ -1077,12 +1095,22 @@ static cudaError_t launch_step_kernel(const Arena& a, const CUtensorMap& map, bo
         prefer_l1(step_kernel<false, true, THREADS>);
     }
     const unsigned blocks = blocks_for(a.nslots, THREADS);
+    Arena r = a;
+#if VLJ_STEP_REMAP
+    static int per_sm = 0;
+    if (!per_sm &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel<true, false, THREADS>,
+                                                      THREADS, 0) != cudaSuccess)
+        per_sm = 0;
+    r.remap_sms = (uint32_t)sm_count();
+    r.remap_per_sm = (uint32_t)per_sm;
+#endif
     if (shifted_force) {
-        if (heat) step_kernel<true, true, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
-        else step_kernel<true, false, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+        if (heat) step_kernel<true, true, THREADS><<<blocks, THREADS, 0, s>>>(r, map, next);
+        else step_kernel<true, false, THREADS><<<blocks, THREADS, 0, s>>>(r, map, next);
     } else {
-        if (heat) step_kernel<false, true, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
-        else step_kernel<false, false, THREADS><<<blocks, THREADS, 0, s>>>(a, map, next);
+        if (heat) step_kernel<false, true, THREADS><<<blocks, THREADS, 0, s>>>(r, map, next);
+        else step_kernel<false, false, THREADS><<<blocks, THREADS, 0, s>>>(r, map, next);
     }
     return after_launch();
 }

@@ -74,6 +74,11 @@ constexpr int kSlots = 8;  // measurement accumulators per box
 #ifndef VLJ_TILE_F32
 #define VLJ_TILE_F32 0
 #endif
+// 1: the step kernel's blocks that share an SM take neighbouring runs of
+// particles (their neighbourhoods overlap in that SM's L1)
+#ifndef VLJ_STEP_REMAP
+#define VLJ_STEP_REMAP 0
+#endif
 #ifndef VLJ_TILE_PIPE
 #define VLJ_TILE_PIPE 0
 #endif
@@ -248,6 +253,7 @@ struct Arena {
     uint32_t tile_cap;   // tile entries (16 B each) a block stages in shared memory
     uint32_t tile_threads;  // threads of a tile step block
     uint32_t step_threads;  // particles per block of the step kernel: 64, 128 or 256
+    uint32_t remap_sms, remap_per_sm;  // the step kernel's first-wave block layout (VLJ_STEP_REMAP)
     // per force block (kForceThreads slots), for the TMA tile ring only: rows
     // (four entries each) of the longest list in it, so a block stages only
     // the rows its particles use. Reset at each rebuild of

@@ -66,6 +66,8 @@ TILE_COLS = (0, 3, 4, 5, 6, 8)
 CANDIDATES = {
     "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
     "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
+    "stream_c4_remap": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4, "VLJ_STEP_REMAP": 1},
+    "stream_c8_remap": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8, "VLJ_STEP_REMAP": 1},
     "stream_c8": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8},
     "ahead_c0": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 0},
     "ahead_c4": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 4},
