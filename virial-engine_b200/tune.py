@@ -41,14 +41,7 @@ OUT_DIR = os.path.join(HERE, "build", "tune")
 # tiles in flight)
 # list-build variants: candidates fetched per round, staged per warp, and the
 # blocks per SM the registers are sized for
-BUILD_# cell-tile variants: compile-time form x bricks per x-row (0: tiles off)
-TILE_CANDIDATES = {
-    "encoded": {},
-    "f32": {"VLJ_TILE_F32": 1},
-    "read_ahead": {"VLJ_TILE_PIPE": 1},
-}
-TILE_COLS = (0, 3, 4, 5, 6, 8)
-CANDIDATES = {
+BUILD_CANDIDATES = {
     "single_stage448_b6": {"VLJ_BUILD_PAIRS": 0},
     "single_stage512_b6": {"VLJ_BUILD_PAIRS": 0, "VLJ_BUILD_STAGE": 512},
     "pairs_stage448_b6": {},
@@ -66,12 +59,10 @@ TILE_COLS = (0, 3, 4, 5, 6, 8)
 CANDIDATES = {
     "stream_c0": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 0},
     "stream_c4": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4},
+    "stream_c8": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8},
     "stream_c4_remap": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 4, "VLJ_STEP_REMAP": 1},
     "stream_c8_remap": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8, "VLJ_STEP_REMAP": 1},
-    "stream_c8": {"VLJ_LIST_STREAM": 1, "VLJ_L1_CARVEOUT": 8},
-    "ahead_c0": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 0},
     "ahead_c4": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 4},
-    "ahead_c8": {"VLJ_LIST_STREAM": 1, "VLJ_GATHER_AHEAD": 1, "VLJ_L1_CARVEOUT": 8},
     "tma_r1_s4": {"VLJ_LIST_STREAM": 0, "VLJ_TILE_ROWS": 1, "VLJ_TILE_SLOTS": 4},
 }
 
