@@ -1142,11 +1142,15 @@ cudaError_t launch_step(const Arena& a, const CUtensorMap& map, bool shifted_for
         return heat ? launch_tile_step<false, true>(a, s, next)
                     : launch_tile_step<false, false>(a, s, next);
     }
-    switch (VLJ_LIST_STREAM ? a.step_threads : (uint32_t)kForceThreads) {
+#if VLJ_LIST_STREAM
+    switch (a.step_threads) {
         case 64: return launch_step_kernel<64>(a, map, shifted_force, s, next, heat);
         case 256: return launch_step_kernel<256>(a, map, shifted_force, s, next, heat);
         default: return launch_step_kernel<kForceThreads>(a, map, shifted_force, s, next, heat);
     }
+#else
+    return launch_step_kernel<kForceThreads>(a, map, shifted_force, s, next, heat);
+#endif
 }
 
 cudaError_t launch_measure(const Arena& a, const CUtensorMap& map, bool shifted_force,
