@@ -41,7 +41,7 @@ namespace vlj {
 #define VLJ_BUILD_ROUND 128
 #endif
 #ifndef VLJ_BUILD_STAGE
-#define VLJ_BUILD_STAGE 448
+#define VLJ_BUILD_STAGE 512
 #endif
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
@@ -49,11 +49,14 @@ namespace vlj {
 // 1: in boxes of five or more cells a side, the test takes two home
 // particles at a time
 #ifndef VLJ_BUILD_PAIRS
-#define VLJ_BUILD_PAIRS 1
+#define VLJ_BUILD_PAIRS 0
 #endif
 constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
 constexpr int kRound = VLJ_BUILD_ROUND;
 constexpr int kStage = VLJ_BUILD_STAGE;
+// with the cell tiles' 16-bit lists the staged candidates also carry their
+// tile indices, so fewer fit beside them
+constexpr int kStageTiles = kStage - 64;
 constexpr int kBuildBlocksPerSM = VLJ_BUILD_BLOCKS_PER_SM;
 static_assert(kRound % 32 == 0 && kStage % 32 == 0 && kRound <= kStage, "build stage shape");
 
@@ -111,7 +114,11 @@ __device__ __forceinline__ bool repeats(int32_t d, int32_t n) {
     return (n == 2 && d == 1) || (n == 1 && d != 0);
 }
 
+// TILES: also write the 16-bit tile lists of the cell-tile step kernel (a
+// box with bricks; the instantiation without it carries none of their work).
+template <bool TILES>
 __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_list_kernel(Arena a) {
+    constexpr int kStage = TILES ? kStageTiles : vlj::kStage;
     count_kernel(a);
     if (!a.glob->any) return;
     __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
@@ -119,7 +126,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     // (wide boxes) or as encoded words (narrow ones), the slot in w
     __shared__ uint4 s_cand[kBuildWarps][kStage];
     // with cell tiles: each staged candidate's index in the brick's tile
-    __shared__ uint16_t s_tix[kBuildWarps][kStage];
+    __shared__ uint16_t s_tix[kBuildWarps][TILES ? kStage : 1];
     __shared__ uint4 s_home[kBuildWarps][32];
     for (int t = threadIdx.x; t < 512; t += blockDim.x)
         s_q510[t] = __fdiv_rn((float)(t - 256), 510.0f);
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
         // With cell tiles: lane s's stencil cell's first particle's index in
         // the tile of the home cell's brick (tile_step_kernel stages the same
         // tile), and the home cell's own (stencil lane 13).
-        const bool tiles = a.list16 != nullptr && bx.brick_cols != 0u;
+        const bool tiles = TILES && bx.brick_cols != 0u;
         uint32_t tbase = 0;
         if (tiles) {
             const Brick k = make_brick(bx, brick_col_of(bx, (uint32_t)c[0]), (uint32_t)c[1],
@@ -276,7 +283,8 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                     const uint32_t from = __shfl_sync(0xffffffffu, cs, lo);
                     const uint32_t at = __shfl_sync(0xffffffffu, off, lo);
                     j[r] = t < total ? a.sorted[from + t - at] : 0xffffffffu;
-                    tix[r] = __shfl_sync(0xffffffffu, tbase, lo) + t - at;
+                    // (tiles is the same for the whole warp)
+                    if (tiles) tix[r] = __shfl_sync(0xffffffffu, tbase, lo) + t - at;
                 }
                 uint4 pe[kRound / 32];
 #pragma unroll
@@ -460,7 +468,11 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
 }
 
 cudaError_t launch_build_list(const Arena& a, cudaStream_t s) {
-    build_list_kernel<<<(unsigned)sm_count() * kBuildBlocksPerSM, kBuildWarps * 32, 0, s>>>(a);
+    const unsigned blocks = (unsigned)sm_count() * kBuildBlocksPerSM;
+    if (a.list16)
+        build_list_kernel<true><<<blocks, kBuildWarps * 32, 0, s>>>(a);
+    else
+        build_list_kernel<false><<<blocks, kBuildWarps * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -42,12 +42,11 @@ OUT_DIR = os.path.join(HERE, "build", "tune")
 # list-build variants: candidates fetched per round, staged per warp, and the
 # blocks per SM the registers are sized for
 BUILD_CANDIDATES = {
-    "single_stage448_b6": {"VLJ_BUILD_PAIRS": 0},
-    "single_stage512_b6": {"VLJ_BUILD_PAIRS": 0, "VLJ_BUILD_STAGE": 512},
-    "pairs_stage448_b6": {},
-    "pairs_stage448_b5": {"VLJ_BUILD_PAIRS": 1, "VLJ_BUILD_BLOCKS_PER_SM": 5},
-    "pairs_stage384_b7": {"VLJ_BUILD_PAIRS": 1, "VLJ_BUILD_STAGE": 384,
-                          "VLJ_BUILD_BLOCKS_PER_SM": 7},
+    "single_stage512_b6": {},
+    "single_stage448_b6": {"VLJ_BUILD_STAGE": 448},
+    "pairs_stage512_b6": {"VLJ_BUILD_PAIRS": 1},
+    "pairs_stage448_b6": {"VLJ_BUILD_PAIRS": 1, "VLJ_BUILD_STAGE": 448},
+    "single_stage512_b5": {"VLJ_BUILD_BLOCKS_PER_SM": 5},
 }
 # cell-tile variants: compile-time form x bricks per x-row (0: tiles off)
 TILE_CANDIDATES = {
