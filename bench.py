@@ -413,6 +413,51 @@ def run_slab(args, world, rank, stream, flush_l2):
                       "list_grows": m.list_grows}}
 
 
+def run_small(args, world, rank, stream, flush_l2):
+    """The small plain box in full: 1000 atoms on the reference's lattice()
+    at rho 0.8442 (box 10.58; fcc 5^3 x 4 holds only 500, in a box under three
+    cutoff + skin wide), truncated-shifted, Maxwell-Boltzmann at T = 0.72,
+    constant energy, dt 0.005, 1000 steps, timed as one enqueue of the 1000
+    steps (L2 flushed before it; the box's 100 KB stays in L2 for the run,
+    as in any run of it), with PE, KE, virial, pressure and the drift of E
+    per particle."""
+    import torch
+    import virial_lj as vl
+
+    n = 1000
+    box = (n / 0.8442) ** (1.0 / 3.0)
+    p = vl.lattice(n, box, 0.72, 1 + rank)
+    st = vl.Settings([box] * 3, cutoff=2.5, dt=0.005, skin=0.3)
+    sim = vl.LennardJones(p, st, stream=stream.cuda_stream)
+    sim.step(50)  # warm-up on a copy, to build the graphs
+    sim.close()
+    sim = vl.LennardJones(p, st, stream=stream.cuda_stream)
+    sim.step(16)
+    m0 = sim.measure_now()
+    stream.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush_l2()
+    e0.record(stream)
+    sim.step(1000)
+    e1.record(stream)
+    stream.synchronize()
+    ms = reduce_max(world, e0.elapsed_time(e1))
+    m1 = sim.measure_now()
+    sim.close()
+    return {"workload": "lj-lattice-1000-rho0.8442-truncated-nve-T0.72-1000-steps",
+            "value": world * n * 1000 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / 1000,
+            "ms_per_run": ms, "steps": 1000,
+            "config": {"dt": 0.005, "cutoff": 2.5, "skin": 0.3, "thermostat": "none",
+                       "launch": "one enqueue of 1000 steps (16-step graphs)",
+                       "l2": "flushed before the run"},
+            "readouts": {"potential_per_particle": m1.potential / n,
+                         "kinetic_per_particle": m1.kinetic / n,
+                         "virial_per_particle": m1.virial / n, "pressure": m1.pressure(),
+                         "drift_per_particle": (m1.energy() - m0.energy()) / n,
+                         "list_rebuilds": m1.list_rebuilds}}
+
+
 def run_heat_flux(args, world, rank, stream):
     """The large constant-energy box with the heat current sampled every step:
     16,384,000 atoms (fcc 160^3 x 4, rho 0.8442), truncated-shifted, dt 0.004.
@@ -546,6 +591,7 @@ def run_ours(args, world, rank, gpu_index):
     batched = run_batched(args, world, rank, stream, flush_l2, peak, fp32_peak)
     heat_flux = run_heat_flux(args, world, rank, stream)
     slab = run_slab(args, world, rank, stream, flush_l2)
+    small = run_small(args, world, rank, stream, flush_l2)
     clk = clocks.stop() if rank == 0 else None
 
     # ---- end to end through the C ABI with host buffers (pinned) ----
@@ -599,6 +645,7 @@ def run_ours(args, world, rank, gpu_index):
             "batched": batched,
             "heat_flux": heat_flux,
             "slab": slab,
+            "small_box": small,
             "clocks": clk,
             "gpu_launches": launches,
             "list_rebuilds_timed": rebuilds,

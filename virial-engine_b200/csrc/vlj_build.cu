@@ -46,10 +46,12 @@ namespace vlj {
 #ifndef VLJ_BUILD_BLOCKS_PER_SM
 #define VLJ_BUILD_BLOCKS_PER_SM 6
 #endif
-// 1: in boxes of five or more cells a side, the test takes two home
-// particles at a time
-#ifndef VLJ_BUILD_PAIRS
-#define VLJ_BUILD_PAIRS 0
+// 0: the test walks the staged candidates' groups outermost, each against
+// every home particle; 1: the home particles outermost, each over all staged
+// candidates (more instructions: 147 M against 142 M for the 256k box's full
+// build)
+#ifndef VLJ_BUILD_ORDER
+#define VLJ_BUILD_ORDER 0
 #endif
 constexpr int kBuildWarps = 4;  // warps per block, each building one home cell at a time
 constexpr int kRound = VLJ_BUILD_ROUND;
@@ -326,112 +328,98 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 // another round
                 if (base + kRound < total && staged + kRound <= (uint32_t)kStage) continue;
                 __syncwarp();
-                // Test: 32 staged candidates at a time, a lane each, against
-                // every home particle in turn. The lanes that accept write
-                // their candidates into that home particle's list themselves,
-                // in stream order (its count so far plus the rank in the
-                // ballot), so every lane is busy whatever the cell's
-                // occupancy and however unevenly the homes accept. Candidates
-                // in the thin shell between the two radii take the
-                // reference's test.
+                // Test: every home particle in turn against the staged
+                // candidates, 32 at a time, a lane each. The lanes that
+                // accept write their candidates into that home particle's
+                // list themselves, in stream order (its count so far plus
+                // their rank in the ballot), so every lane is busy whatever
+                // the cell's occupancy and however unevenly the homes
+                // accept. Candidates in the thin shell between the two radii
+                // take the reference's test.
+#if VLJ_BUILD_ORDER == 0
+                // The candidates' group is the outer loop, the homes' counts
+                // in their lanes.
                 for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
                     const uint32_t q = c0 + lane;
                     const bool valid = q < staged;
                     const uint4 e = s_cand[warp][valid ? q : 0u];
                     const uint32_t e_tix = tiles ? s_tix[warp][valid ? q : 0u] : 0u;
-                    auto settle = [&](uint32_t h, uint32_t home_slot, float r2e) {
-                        const bool near = valid && r2e < pre_r2 && e.w != home_slot;
+                    for (uint32_t h = 0; h < homes; h++) {
+                        const uint4 hp = s_home[warp][h];
+                        float r2e;
+                        if (wide) {
+                            const float dx = __uint_as_float(e.x) - __uint_as_float(hp.x);
+                            const float dy = __uint_as_float(e.y) - __uint_as_float(hp.y);
+                            const float dz = __uint_as_float(e.z) - __uint_as_float(hp.z);
+                            r2e = dx * dx + dy * dy + dz * dz;
+                        } else {
+                            r2e = encoded_r2(e, hp, dec);
+                        }
+                        const bool near = valid && r2e < pre_r2 && e.w != hp.w;
                         bool take = near && r2e < acc_r2;
-                        if (near && !take) take = ref_test(a, bx, home_slot, e.w, s_q510);
+                        if (near && !take) take = ref_test(a, bx, hp.w, e.w, s_q510);
                         const unsigned m = __ballot_sync(0xffffffffu, take);
-                        if (m == 0u) return;
+                        if (m == 0u) continue;
                         const uint32_t k = __shfl_sync(0xffffffffu, found, h) +
                                            (uint32_t)__popc(m & below);
-                        // entry k of the home particle's list: row k / 4, place k % 4
                         store_if(take && k < cap,
                                  a.list + ((unsigned long long)(k >> 2) * row_stride +
-                                           (home_slot * 4u + (k & 3u))),
+                                           (hp.w * 4u + (k & 3u))),
                                  e.w);
-                        // entry k of the 16-bit list of the home's sorted
-                        // position h0 + h: row k / 8, place k % 8
                         if (tiles)
                             store16_if(take && k < cap,
                                        a.list16 + ((unsigned long long)(k >> 3) * row16_stride +
                                                    ((h0 + h) * 8u + (k & 7u))),
                                        e_tix);
                         if (lane == h) found += (uint32_t)__popc(m);
-                    };
-#if VLJ_BUILD_PAIRS
-                    if (wide) {
-                        // two home particles at a time: their tests are
-                        // independent, so each one's dependent chain of
-                        // arithmetic, votes and stores fills the other's gaps
-                        const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
-                                    ez = __uint_as_float(e.z);
-                        for (uint32_t h = 0; h < homes; h += 2) {
-                            const bool two = h + 1u < homes;
-                            const uint32_t h1 = two ? h + 1u : h;
-                            const uint4 pa = s_home[warp][h], pb = s_home[warp][h1];
-                            const float ax = ex - __uint_as_float(pa.x), bx_ = ex - __uint_as_float(pb.x);
-                            const float ay = ey - __uint_as_float(pa.y), by = ey - __uint_as_float(pb.y);
-                            const float az = ez - __uint_as_float(pa.z), bz = ez - __uint_as_float(pb.z);
-                            const float ra = ax * ax + ay * ay + az * az;
-                            const float rb = bx_ * bx_ + by * by + bz * bz;
-                            const bool near_a = valid && ra < pre_r2 && e.w != pa.w;
-                            const bool near_b = two && valid && rb < pre_r2 && e.w != pb.w;
-                            bool take_a = near_a && ra < acc_r2;
-                            bool take_b = near_b && rb < acc_r2;
-                            if (near_a && !take_a) take_a = ref_test(a, bx, pa.w, e.w, s_q510);
-                            if (near_b && !take_b) take_b = ref_test(a, bx, pb.w, e.w, s_q510);
-                            const unsigned ma = __ballot_sync(0xffffffffu, take_a);
-                            const unsigned mb = __ballot_sync(0xffffffffu, take_b);
-                            if ((ma | mb) == 0u) continue;
-                            const uint32_t ka = __shfl_sync(0xffffffffu, found, h) +
-                                                (uint32_t)__popc(ma & below);
-                            const uint32_t kb = __shfl_sync(0xffffffffu, found, h1) +
-                                                (uint32_t)__popc(mb & below);
-                            store_if(take_a && ka < cap,
-                                     a.list + ((unsigned long long)(ka >> 2) * row_stride +
-                                               (pa.w * 4u + (ka & 3u))),
-                                     e.w);
-                            store_if(take_b && kb < cap,
-                                     a.list + ((unsigned long long)(kb >> 2) * row_stride +
-                                               (pb.w * 4u + (kb & 3u))),
-                                     e.w);
-                            if (tiles) {
-                                store16_if(take_a && ka < cap,
-                                           a.list16 + ((unsigned long long)(ka >> 3) * row16_stride +
-                                                       ((h0 + h) * 8u + (ka & 7u))),
-                                           e_tix);
-                                store16_if(take_b && kb < cap,
-                                           a.list16 + ((unsigned long long)(kb >> 3) * row16_stride +
-                                                       ((h0 + h1) * 8u + (kb & 7u))),
-                                           e_tix);
-                            }
-                            if (lane == h) found += (uint32_t)__popc(ma);
-                            if (two && lane == h1) found += (uint32_t)__popc(mb);
-                        }
-                    } else
-#else
-                    if (wide) {
-                        const float ex = __uint_as_float(e.x), ey = __uint_as_float(e.y),
-                                    ez = __uint_as_float(e.z);
-                        for (uint32_t h = 0; h < homes; h++) {
-                            const uint4 hp = s_home[warp][h];
-                            const float dx = ex - __uint_as_float(hp.x);
-                            const float dy = ey - __uint_as_float(hp.y);
-                            const float dz = ez - __uint_as_float(hp.z);
-                            settle(h, hp.w, dx * dx + dy * dy + dz * dz);
-                        }
-                    } else
-#endif
-                    {
-                        for (uint32_t h = 0; h < homes; h++) {
-                            const uint4 hp = s_home[warp][h];
-                            settle(h, hp.w, encoded_r2(e, hp, dec));
-                        }
                     }
                 }
+#else
+                // The home is the outer loop: its position and its count so
+                // far sit in warp-uniform registers for all its groups.
+                auto test_homes = [&](auto r2_of) {
+                    for (uint32_t h = 0; h < homes; h++) {
+                        const uint4 hp = s_home[warp][h];
+                        uint32_t fh = __shfl_sync(0xffffffffu, found, h);
+                        uint32_t* const row0 = a.list + (size_t)hp.w * 4u;
+                        uint16_t* const row16 = tiles ? a.list16 + (size_t)(h0 + h) * 8u : nullptr;
+                        for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
+                            const uint32_t q = c0 + lane;
+                            const bool valid = q < staged;
+                            const uint4 e = s_cand[warp][valid ? q : 0u];
+                            const float r2e = r2_of(e, hp);
+                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
+                            bool take = near && r2e < acc_r2;
+                            if (near && !take) take = ref_test(a, bx, hp.w, e.w, s_q510);
+                            const unsigned m = __ballot_sync(0xffffffffu, take);
+                            // (most groups of a home on the far side of the
+                            // stencil take nothing)
+                            if (m == 0u) continue;
+                            // entry k of the home particle's list: row k / 4, place k % 4
+                            const uint32_t k = fh + (uint32_t)__popc(m & below);
+                            store_if(take && k < cap, row0 + ((size_t)(k >> 2) * row_stride + (k & 3u)),
+                                     e.w);
+                            // entry k of the 16-bit list of the home's sorted
+                            // position h0 + h: row k / 8, place k % 8
+                            if (tiles)
+                                store16_if(take && k < cap,
+                                           row16 + ((size_t)(k >> 3) * row16_stride + (k & 7u)),
+                                           s_tix[warp][valid ? q : 0u]);
+                            fh += (uint32_t)__popc(m);
+                        }
+                        if (lane == h) found = fh;
+                    }
+                };
+                if (wide)
+                    test_homes([&](const uint4& e, const uint4& hp) {
+                        const float dx = __uint_as_float(e.x) - __uint_as_float(hp.x);
+                        const float dy = __uint_as_float(e.y) - __uint_as_float(hp.y);
+                        const float dz = __uint_as_float(e.z) - __uint_as_float(hp.z);
+                        return dx * dx + dy * dy + dz * dz;
+                    });
+                else
+                    test_homes([&](const uint4& e, const uint4& hp) { return encoded_r2(e, hp, dec); });
+#endif
                 __syncwarp();
                 staged = 0;
             }

@@ -161,12 +161,17 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(Arena a) {
         // the runs that reach into the box (warp-uniform; a small box has
         // fewer cells than one pass covers)
         const uint32_t runs = first >= total ? 0u : min((uint32_t)kScanPer, (total - first + 31u) / 32u);
+        // every run's count is read before the first shuffle, so the warp
+        // waits for the loads once rather than once a run
 #pragma unroll
         for (int r = 0; r < kScanPer; r++) {
-            excl[r] = 0u;
-            if ((uint32_t)r >= runs) continue;
             const uint32_t c = first + 32u * (uint32_t)r + lane;
-            const uint32_t v = c < total ? a.count[base + c] : 0u;
+            excl[r] = c < total ? a.count[base + c] : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < kScanPer; r++) {
+            if ((uint32_t)r >= runs) continue;
+            const uint32_t v = excl[r];
             uint32_t x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -290,71 +295,125 @@ __device__ __forceinline__ void move_to_scratch(const Arena& a, uint32_t from, u
     a.scell[to] = cell;
 }
 
-__global__ void sort_kernel(Arena a) {
+// A cell of more than 32 particles: ranks in registers up to 32 * kSortRegs,
+// else (improbably full cells) lane 0's insertion sort, as the reference.
+__device__ __forceinline__ void sort_big_cell(const Arena& a, uint32_t cell, uint32_t start,
+                                              uint32_t m, bool reorder, uint32_t lane) {
+    const uint32_t end = start + m;
+    if (m <= 32u * kSortRegs) {
+        uint32_t key[kSortRegs], rank[kSortRegs];
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
+            rank[r] = 0;
+        }
+        for (int rr = 0; rr < kSortRegs; rr++) {
+            if ((uint32_t)rr * 32u >= m) break;
+            for (int src = 0; src < 32; src++) {
+                uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
+#pragma unroll
+                for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < kSortRegs; r++) {
+            uint32_t t = r * 32 + lane;
+            if (t < m) {
+                a.sorted[start + rank[r]] = key[r];
+                if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
+            }
+        }
+    } else if (lane == 0) {
+        for (uint32_t s = start + 1; s < end; s++) {
+            uint32_t key = a.sorted[s];
+            uint32_t t = s;
+            while (t > start && a.sorted[t - 1] > key) {
+                a.sorted[t] = a.sorted[t - 1];
+                t -= 1;
+            }
+            a.sorted[t] = key;
+        }
+        if (reorder)
+            for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 4) sort_kernel(Arena a) {
     count_kernel(a);
     if (!grid_pass(a)) return;
-    const int lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t cells = work_total(a), front = a.glob->work_front;
-    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cells; w += warps) {
-        const uint32_t entry = work_item(a, front, w);
-        if (entry & 7u) continue;  // a cell sorts once, with its first part
-        const uint32_t cell = entry >> 3;
-        const uint32_t b = box_of_cell(a, cell);
-        const bool reorder = a.ctrl[b].reorder != 0u;
-        const uint32_t start = a.cell_start[cell], end = a.cell_start[cell + 1];
-        const uint32_t m = end - start;
-        if (lane == 0) a.count[cell] = 0u;
-        if (m <= 32u) {
-            // the usual cell: one key per lane, ranked against the m keys
-            const uint32_t key = (uint32_t)lane < m ? a.sorted[start + lane] : 0xffffffffu;
-            uint32_t rank = 0;
-            for (uint32_t src = 0; src < m; src++)
-                rank += __shfl_sync(0xffffffffu, key, src) < key ? 1u : 0u;
-            __syncwarp();
-            if ((uint32_t)lane < m) {
-                a.sorted[start + rank] = key;
-                if (reorder) move_to_scratch(a, key, start + rank, cell);
-            }
-        } else if (m <= 32u * kSortRegs) {
-            uint32_t key[kSortRegs], rank[kSortRegs];
+    // A warp takes work entries w and w + warps together, so the two cells'
+    // chains of dependent loads (entry, range, slots, particles) overlap.
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cells; w += 2u * warps) {
+        uint32_t cell[2], start[2] = {0u, 0u}, m[2] = {0u, 0u}, key[2], rank[2] = {0u, 0u};
+        bool live[2], reorder[2] = {false, false};
 #pragma unroll
-            for (int r = 0; r < kSortRegs; r++) {
-                uint32_t t = r * 32 + lane;
-                key[r] = t < m ? a.sorted[start + t] : 0xffffffffu;
-                rank[r] = 0;
-            }
-            for (int rr = 0; rr < kSortRegs; rr++) {
-                if ((uint32_t)rr * 32u >= m) break;
-                for (int src = 0; src < 32; src++) {
-                    uint32_t other = __shfl_sync(0xffffffffu, key[rr], src);
-#pragma unroll
-                    for (int r = 0; r < kSortRegs; r++) rank[r] += other < key[r] ? 1u : 0u;
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < kSortRegs; r++) {
-                uint32_t t = r * 32 + lane;
-                if (t < m) {
-                    a.sorted[start + rank[r]] = key[r];
-                    if (reorder) move_to_scratch(a, key[r], start + rank[r], cell);
-                }
-            }
-        } else if (lane == 0) {
-            // insertion sort, as the reference, for improbably full cells
-            for (uint32_t s = start + 1; s < end; s++) {
-                uint32_t key = a.sorted[s];
-                uint32_t t = s;
-                while (t > start && a.sorted[t - 1] > key) {
-                    a.sorted[t] = a.sorted[t - 1];
-                    t -= 1;
-                }
-                a.sorted[t] = key;
-            }
-            if (reorder)
-                for (uint32_t s = start; s < end; s++) move_to_scratch(a, a.sorted[s], s, cell);
+        for (int k = 0; k < 2; k++) {
+            const uint32_t t = w + (uint32_t)k * warps;
+            const uint32_t entry = t < cells ? work_item(a, front, t) : 1u;
+            live[k] = (entry & 7u) == 0u;  // a cell sorts once, with its first part
+            cell[k] = entry >> 3;
         }
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (live[k]) {
+                start[k] = a.cell_start[cell[k]];
+                m[k] = a.cell_start[cell[k] + 1] - start[k];
+                reorder[k] = a.ctrl[box_of_cell(a, cell[k])].reorder != 0u;
+                if (lane == 0) a.count[cell[k]] = 0u;
+            }
+        // the usual cell: one key per lane, ranked against the m keys (a
+        // lane past m holds the largest key, which ranks below no one)
+        bool small[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            small[k] = live[k] && m[k] <= 32u;
+            key[k] = small[k] && lane < m[k] ? a.sorted[start[k] + lane] : 0xffffffffu;
+        }
+        const uint32_t mm = max(small[0] ? m[0] : 0u, small[1] ? m[1] : 0u);
+        for (uint32_t src = 0; src < mm; src++) {
+            rank[0] += __shfl_sync(0xffffffffu, key[0], src) < key[0] ? 1u : 0u;
+            rank[1] += __shfl_sync(0xffffffffu, key[1], src) < key[1] ? 1u : 0u;
+        }
+        __syncwarp();
+        // with reorder, both cells' particles are read before any is written
+        double px[2][3], pv[2][3];
+        uint32_t pid[2];
+        bool moves[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            moves[k] = small[k] && lane < m[k] && reorder[k];
+            if (moves[k]) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    px[k][d] = a.x[d * a.seg + key[k]];
+                    pv[k][d] = a.v[d * a.seg + key[k]];
+                }
+                pid[k] = a.id[key[k]];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            if (!(small[k] && lane < m[k])) continue;
+            const uint32_t to = start[k] + rank[k];
+            a.sorted[to] = key[k];
+            if (moves[k]) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    a.sx[d * a.seg + to] = px[k][d];
+                    a.sv[d * a.seg + to] = pv[k][d];
+                }
+                a.sid[to] = pid[k];
+                a.scell[to] = cell[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (live[k] && m[k] > 32u) sort_big_cell(a, cell[k], start[k], m[k], reorder[k], lane);
         __syncwarp();
     }
 }

@@ -5,6 +5,7 @@ measure). Also the target of the committed ncu summaries in profiles/.
 
     python virial-engine_b200/examples/lj_box.py --cells 40 --steps 100
     python virial-engine_b200/examples/lj_box.py --cells 10 --steps 1000 --record run1
+    python virial-engine_b200/examples/lj_box.py --lattice 1000 --temperature 0.72 --nve --truncated
 """
 
 import argparse
@@ -20,6 +21,9 @@ import virial_lj as vl  # noqa: E402
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cells", type=int, default=40, help="fcc unit cells per side (4 atoms each)")
+    ap.add_argument("--lattice", type=int, default=0, metavar="N",
+                    help="N atoms on the reference's lattice() in a cube of the density "
+                         "instead of the fcc lattice")
     ap.add_argument("--density", type=float, default=0.8442)
     ap.add_argument("--temperature", type=float, default=1.0)
     ap.add_argument("--steps", type=int, default=100)
@@ -36,7 +40,11 @@ def main():
                          "and run.json into DIR, in the reference's formats")
     ap.add_argument("--every", type=int, default=10)
     args = ap.parse_args()
-    p, box = vl.lattice_fcc(args.cells, args.density, args.temperature, args.seed)
+    if args.lattice:
+        box = (args.lattice / args.density) ** (1.0 / 3.0)
+        p = vl.lattice(args.lattice, box, args.temperature, args.seed)
+    else:
+        p, box = vl.lattice_fcc(args.cells, args.density, args.temperature, args.seed)
     thermostat = None if args.nve else vl.Langevin(args.temperature, 1.0, args.seed)
     sim = vl.LennardJones(p, vl.Settings([box] * 3, dt=args.dt, thermostat=thermostat,
                                          shifted_force=not args.truncated))

@@ -39,14 +39,17 @@ OUT_DIR = os.path.join(HERE, "build", "tune")
 # name -> preprocessor overrides: rows streamed without L1 allocation under
 # shared-memory carve-out hints (percent), or the TMA tile ring (rows per tile,
 # tiles in flight)
-# list-build variants: candidates fetched per round, staged per warp, and the
-# blocks per SM the registers are sized for
+# list-build variants: the test's loop order (home particles or candidate
+# groups outermost), candidates staged per warp, and the blocks per SM the
+# registers are sized for
 BUILD_CANDIDATES = {
-    "single_stage512_b6": {},
-    "single_stage448_b6": {"VLJ_BUILD_STAGE": 448},
-    "pairs_stage512_b6": {"VLJ_BUILD_PAIRS": 1},
-    "pairs_stage448_b6": {"VLJ_BUILD_PAIRS": 1, "VLJ_BUILD_STAGE": 448},
-    "single_stage512_b5": {"VLJ_BUILD_BLOCKS_PER_SM": 5},
+    "groups_outer_stage512_b6": {},
+    "groups_outer_stage448_b6": {"VLJ_BUILD_STAGE": 448},
+    "groups_outer_stage416_b7": {"VLJ_BUILD_STAGE": 416, "VLJ_BUILD_BLOCKS_PER_SM": 7},
+    "groups_outer_stage352_b8": {"VLJ_BUILD_STAGE": 352, "VLJ_BUILD_BLOCKS_PER_SM": 8},
+    "homes_outer_stage512_b6": {"VLJ_BUILD_ORDER": 1},
+    "homes_outer_stage416_b7": {"VLJ_BUILD_ORDER": 1, "VLJ_BUILD_STAGE": 416,
+                                "VLJ_BUILD_BLOCKS_PER_SM": 7},
 }
 # cell-tile variants: compile-time form x bricks per x-row (0: tiles off)
 TILE_CANDIDATES = {
