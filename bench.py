@@ -101,7 +101,7 @@ def profile_traffic():
 
 
 def roofline_line(hbm_achieved, hbm_peak, hbm_kind, fp32_achieved, fp32_peak, fpps, traffic,
-                  avg_kernel_s, launches):
+                  avg_kernel_s, launches, kernel="step_kernel<true>"):
     """The step kernel against the roofline that binds it: the algorithmic
     bytes (96 B per particle-step) over the measured HBM copy bandwidth, or
     the algorithmic FP32 flops over the measured FMA throughput, whichever
@@ -118,7 +118,7 @@ def roofline_line(hbm_achieved, hbm_peak, hbm_kind, fp32_achieved, fp32_peak, fp
     top = fp32 if fp32_binds else hbm
     return {"bound": "fp32" if fp32_binds else "hbm", "achieved": top["achieved"],
             "peak": top["peak"], "unit": top["unit"], "frac": top["frac"], "traffic": traffic,
-            "kernel": "step_kernel<true>", "avg_kernel_us": avg_kernel_s * 1e6,
+            "kernel": kernel, "avg_kernel_us": avg_kernel_s * 1e6,
             "kernel_launches_timed": launches, "hbm": hbm, "fp32": fp32}
 
 
@@ -514,7 +514,12 @@ def run_ours(args, world, rank, gpu_index):
                            thermostat=vl.Langevin(WORK["temperature"], WORK["friction"],
                                                   WORK["seed"] + rank),
                            shifted_force=True, skin=WORK["skin"])
+    # the step kernel's form (cell tiles' bricks per row, particles per
+    # block), timed on a copy of the box; none of them changes the trajectory
+    tile_cols, step_threads, form_times = vl.tune_box(p, settings, stream=stream)
     sim = vl.LennardJones(p, settings, stream=stream.cuda_stream)
+    sim.set_tile_cols(tile_cols)
+    sim.set_step_threads(step_threads)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     def flush_l2():
@@ -632,14 +637,22 @@ def run_ours(args, world, rank, gpu_index):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "state_dtype": "f64",
-            "data": "synthetic", "config": config(n, world),
+            "data": "synthetic",
+            "config": dict(config(n, world), step_form={
+                "tile_cols": tile_cols, "step_threads": step_threads,
+                "tuned_ms_per_step": {f"tiles {c} threads {t}": v * 1e3
+                                      for (c, t), v in form_times.items()},
+                "note": "virial_lj.tune_box on a copy of the box (L2 flushed per step); "
+                        "every form gives the same trajectory to the bit"}),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "note": f"per bench step: write particles from pinned host memory, "
                             f"{E2E_INNER} MD steps, measure_now, read_particles into pinned "
                             "host memory; wall clock"},
             "roofline": roofline_line(achieved, peak, peak_kind, fp32_achieved, fp32_peak, fpps,
-                                      traffic, avg_kernel_s, kern_n),
+                                      traffic, avg_kernel_s, kern_n,
+                                      "tile_step_kernel<true>" if tile_cols
+                                      else f"step_kernel<true, false, {step_threads}>"),
             "cpu_baseline": cpu,
             "grid_every_step": grid_every,
             "batched": batched,

@@ -200,6 +200,18 @@ VLJ_API vlj_status vlj_heat_flux(const vlj_sim *sim, int *has, double *flux);
  * behaviour (from creation on when the environment sets
  * VLJ_LIST_GROWTH=0). */
 VLJ_API vlj_status vlj_set_list_growth(vlj_sim *sim, int on);
+/* No reference counterpart: the step kernel's cell tiles of a single box at
+ * run time (a tuning knob, virial_lj.tune_box). cols >= 1: bricks of whole
+ * cells along x, `cols` bricks per x-row (at most the cells along x), each
+ * block staging its brick's neighbour rows in shared memory; 0: the
+ * per-particle gathers from the slot list (the default). The trajectory is
+ * the same to the bit either way. Waits for the stream; the tiles take over
+ * at the next list rebuild the skin schedule brings (which builds their
+ * 16-bit lists beside the slot lists: a rebuild out of turn would change
+ * the trajectory's bits), the slot lists until then. VLJ_INVALID_ARG for a
+ * batch's simulation, or cols >= 1 in a box of fewer than four particles per
+ * cell on average. */
+VLJ_API vlj_status vlj_set_tile_cols(vlj_sim *sim, uint32_t cols);
 /* No reference counterpart (the reference bins only when the lists rebuild):
  * with on != 0, rebuild the cell grid (bin, scan, scatter, per-cell sort) on
  * every step, the Verlet lists still on the skin / 2 trigger. Same trajectory

@@ -306,6 +306,11 @@ vlj_sim::~vlj_sim() {
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
+namespace vlj {
+static bool plan_tiles(Box& b, Arena& a, uint32_t want_cols);  // below
+static vlj_status free_device(vlj_sim* s, void* p);
+}  // namespace vlj
+
 extern "C" {
 
 vlj_status vlj_device_count(int* count) {
@@ -811,6 +816,46 @@ vlj_status vlj_debug_set_tiles(vlj_sim* s, int on) {
     return VLJ_OK;
 }
 
+vlj_status vlj_set_tile_cols(vlj_sim* s, uint32_t cols) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (!s->replicas.empty()) return fail(VLJ_INVALID_ARG, "cell tiles are for a single box");
+    if (cols > s->box.cells[0])
+        return fail(VLJ_INVALID_ARG, "at most %u bricks per x-row (cells along x)", s->box.cells[0]);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    Arena& a = s->arena;
+    Box b = s->box;
+    Arena plan = a;
+    if (cols == 0u) {
+        // per-particle gathers again; the 16-bit lists are no longer built
+        b.brick_cols = b.brick_base = 0u;
+        plan.bricks = plan.tile_cap = plan.tile_threads = 0u;
+        if (a.list16) TRY(free_device(s, a.list16));
+        a.list16 = nullptr;
+    } else {
+        if (!plan_tiles(b, plan, cols))
+            return fail(VLJ_INVALID_ARG, "cell tiles need four or more particles per cell on average");
+        if (!a.list16)
+            TRY(dalloc(s, &a.list16, (size_t)a.seg * 8 * ((b.capacity + 7) / 8)));
+    }
+    a.bricks = plan.bricks;
+    a.tile_cap = plan.tile_cap;
+    a.tile_threads = plan.tile_threads;
+    s->box = b;
+    CUDA_TRY(cudaMemcpy(const_cast<Box*>(a.boxes), &b, sizeof(Box), cudaMemcpyHostToDevice));
+    s->tiles_on = cols != 0u;
+    // No rebuild here: one out of turn would move the reorder schedule and
+    // with it the slot order, the list order and the trajectory's bits. The
+    // tile step kernel walks the slot lists until the next scheduled build
+    // writes the tiles' 16-bit lists for these bricks.
+    const uint32_t zero = 0u;
+    CUDA_TRY(cudaMemcpy(&a.glob->tiles_ready, &zero, sizeof zero, cudaMemcpyHostToDevice));
+    // the captured graphs hold the old arena
+    sim_drop_step_graphs(s);
+    if (s->graph_lists) cudaGraphExecDestroy(s->graph_lists);
+    s->graph_lists = nullptr;
+    return VLJ_OK;
+}
+
 vlj_status vlj_debug_set_step_threads(vlj_sim* s, uint32_t threads) {
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
     if (threads != 64 && threads != 128 && threads != 256)
@@ -941,12 +986,12 @@ vlj_status sim_lists_now(vlj_sim* s) { return lists_now(s); }
 // by default: on the 256,000-atom box the tiles' shared-memory gathers (about
 // 11 bank wavefronts per warp-wide 16-byte load) and their staging measured
 // 75-88 us a step against 51 us for the per-particle gathers through L1.
-static bool plan_tiles(Box& b, Arena& a) {
+// want_cols: the bricks per x-row, or 0 for the size above (VLJ_TILE_COLS
+// at creation, vlj_set_tile_cols at run time).
+static bool plan_tiles(Box& b, Arena& a, uint32_t want_cols) {
     b.brick_cols = 0u;
     b.brick_base = 0u;
     a.bricks = a.tile_cap = a.tile_threads = 0u;
-    const char* env = std::getenv("VLJ_TILES");
-    if (!env || env[0] != '1') return false;
     const double cells = (double)b.total_cells;
     const double mean = (double)b.n / cells;
     if (mean < 4.0) return false;
@@ -954,11 +999,7 @@ static bool plan_tiles(Box& b, Arena& a) {
     const uint32_t nx = b.cells[0];
     const double width = std::max(1.0, std::round(112.0 / occupancy));
     uint32_t cols = (uint32_t)std::ceil((double)nx / width);
-    // VLJ_TILE_COLS sets the bricks per x-row (a tuning knob)
-    if (const char* c = std::getenv("VLJ_TILE_COLS")) {
-        const long v = std::strtol(c, nullptr, 10);
-        if (v >= 1 && v <= (long)nx) cols = (uint32_t)v;
-    }
+    if (want_cols >= 1u) cols = want_cols;
     cols = std::max(1u, std::min(cols, nx));
     // each tile row holds distinct cells: w + 2 <= nx, or one brick per row
     while (cols > 1u && (nx + cols - 1u) / cols + 2u > nx) cols++;
@@ -1068,7 +1109,14 @@ vlj_status sim_allocate(vlj_sim* s, void* stream) {
     TRY(dalloc(s, &a.rb_first, boxes.size() + 1));
     TRY(dalloc(s, &a.list_count, seg));
     TRY(dalloc(s, &a.list, (size_t)seg * 4 * ((cap + 3) / 4)));
-    if (!batched && plan_tiles(s->box, a)) {
+    // VLJ_TILES=1: cell tiles from creation on, VLJ_TILE_COLS bricks per x-row
+    const char* tiles_env = std::getenv("VLJ_TILES");
+    uint32_t env_cols = 0u;
+    if (const char* c = std::getenv("VLJ_TILE_COLS")) {
+        const long v = std::strtol(c, nullptr, 10);
+        if (v >= 1 && v <= 4096) env_cols = (uint32_t)v;
+    }
+    if (!batched && tiles_env && tiles_env[0] == '1' && plan_tiles(s->box, a, env_cols)) {
         TRY(dalloc(s, &a.list16, (size_t)seg * 8 * ((cap + 7) / 8)));
         boxes[0] = s->box;
     }
@@ -1328,6 +1376,17 @@ vlj_status sim_flush_heat(vlj_sim* s) {
     TRY(lists_now(s));
     CUDA_TRY(launch_heat_current(s->arena, s->shifted_force, s->series_samples - 1u, s->stream));
     return VLJ_OK;
+}
+
+// Frees device allocation `p` (one of s->allocations).
+static vlj_status free_device(vlj_sim* s, void* p) {
+    for (size_t k = 0; k < s->allocations.size(); k++)
+        if (s->allocations[k] == p) {
+            s->allocations.erase(s->allocations.begin() + (long)k);
+            CUDA_TRY(cudaFree(p));
+            return VLJ_OK;
+        }
+    return fail(VLJ_INVALID_ARG, "not an allocation of this sim");
 }
 
 // Replaces device allocation `old` (one of s->allocations) by a new one of

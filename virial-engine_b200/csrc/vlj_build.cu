@@ -123,6 +123,8 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
     constexpr int kStage = TILES ? kStageTiles : vlj::kStage;
     count_kernel(a);
     if (!a.glob->any) return;
+    // the tile step kernel reads the 16-bit lists from the next step on
+    if (TILES && blockIdx.x == 0 && threadIdx.x == 0) a.glob->tiles_ready = 1u;
     __shared__ float s_q510[512];  // q / 510 for q = -256..255, IEEE quotients
     // staged candidates: (x, y, z) as f32 offsets from the home cell's centre
     // (wide boxes) or as encoded words (narrow ones), the slot in w

@@ -569,7 +569,9 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
     }
     __syncthreads();
     const uint32_t tile_size = s_base[9];
-    const bool staged = tile_size <= a.tile_cap;
+    // until a build has written the tile lists for these bricks (tiles just
+    // switched on or resized), every block takes the slot list
+    const bool staged = tile_size <= a.tile_cap && a.glob->tiles_ready != 0u;
 #if VLJ_TILE_F32
     // the tile as f32 offsets from the brick's centre (encoded)
     const uint32_t org[3] = {

@@ -168,7 +168,7 @@ struct Global {
     uint32_t rb_slots;           // their particles, in all
     uint32_t heat_next;          // heat-current samples written to the series so far
     uint32_t decided;            // a step kernel took the next step's decision, not yet consumed
-    uint32_t pad;
+    uint32_t tiles_ready;        // the 16-bit tile lists match the box's bricks (a build wrote them)
 };
 
 // Nose-Hoover state of a box (Tuckerman's splitting, lennard_jones.wgsl:309-397).

@@ -29,7 +29,7 @@ __all__ = [
     "PARTICLE", "VljError", "Langevin", "NoseHoover", "Settings", "Measurement", "Slab", "Profile",
     "Phase", "Drawn", "HeatExchange", "LennardJones", "Batch", "Replica", "lattice", "lattice_box",
     "lattice_fcc", "particles", "device_count", "library_path", "launches", "uneven_replicas",
-    "replica_cost", "shard_replicas", "tune_batch_skin", "tune_batch", "grain_cells",
+    "replica_cost", "shard_replicas", "tune_batch_skin", "tune_batch", "tune_box", "grain_cells",
     "grain_contacts",
 ]
 
@@ -445,6 +445,13 @@ class LennardJones:
         the reference's report-only behaviour)."""
         _check(_lib.vlj_set_list_growth(self._h, int(bool(on))))
 
+    def set_tile_cols(self, cols):
+        """Cell tiles in the step kernel at run time: `cols` bricks per x-row
+        (each block stages its brick's neighbour rows in shared memory), or 0
+        for the per-particle gathers (the default). Same trajectory either
+        way; the tiles take over at the next scheduled list rebuild."""
+        _check(_lib.vlj_set_tile_cols(self._h, int(cols)))
+
     def set_grid_every_step(self, on):
         """Rebuild the cell grid on every step as well (the lists still on the
         skin / 2 trigger): the same trajectory, more work per step. Not in the
@@ -777,6 +784,56 @@ def tune_batch(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), threads=(64, 128, 256)
         b.close()
     skin, t = min(times, key=times.get)
     return skin, t, times
+
+
+def tune_box(particles, settings: Settings, tile_cols=(0, 3, 4, 5, 6), threads=(64, 128, 256),
+             steps=30, warmup=10, flush_bytes=256 << 20, stream=None):
+    """The step kernel's form that steps this box fastest on this GPU: the
+    cell tiles' bricks per x-row (0: per-particle gathers, the default) and
+    the particles per block of the per-particle kernel.
+
+    Neither changes the trajectory, so the choice carries over to the box
+    itself. A copy of the box (the same particles and settings) runs every
+    candidate: `warmup` steps, then `steps` single steps timed with CUDA events
+    on `stream` (a torch stream), each after a write of `flush_bytes` that
+    clears the L2 (0: no flush). Tile sizes the box cannot take (too few
+    particles per cell, more bricks than cells along x) are skipped. Returns
+    (cols, threads, {(cols, threads): seconds per step}); apply them with
+    set_tile_cols and set_step_threads.
+    """
+    import torch
+
+    s = stream or torch.cuda.current_stream()
+    flush = torch.empty(max(int(flush_bytes), 1), dtype=torch.uint8, device="cuda")
+    sim = LennardJones(particles, settings, stream=s.cuda_stream)
+    times = {}
+    try:
+        sim.step(warmup)
+        candidates = [(0, t) for t in threads] + [(c, 128) for c in tile_cols if c]
+        for cols, t in candidates:
+            try:
+                sim.set_tile_cols(cols)
+            except VljError:
+                continue
+            sim.set_step_threads(t)
+            if cols:
+                sim.force_rebuild()  # the copy's schedule does not matter: tiles from now on
+            sim.step(3)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(steps)]
+            for a, b in ev:
+                if flush_bytes:
+                    with torch.cuda.stream(s):
+                        flush.fill_(1)
+                a.record(s)
+                sim.step(1)
+                b.record(s)
+            s.synchronize()
+            times[(cols, t)] = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / steps
+    finally:
+        sim.close()
+    cols, t = min(times, key=times.get)
+    return cols, t, times
 
 
 def tune_batch_skin(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), cutoff=2.5, dt=0.005,

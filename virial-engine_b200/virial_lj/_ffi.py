@@ -86,6 +86,7 @@ SIGNATURES = {
     "vlj_heat_flux": [_vp, _P(C.c_int), _P(C.c_double)],
     "vlj_set_grid_every_step": [_vp, C.c_int],
     "vlj_set_list_growth": [_vp, C.c_int],
+    "vlj_set_tile_cols": [_vp, C.c_uint32],
     "vlj_sample_profile": [_vp],
     "vlj_clear_profile": [_vp],
     "vlj_read_profile": [_vp, _P(Slab), _P(C.c_double), _P(C.c_uint64)],
