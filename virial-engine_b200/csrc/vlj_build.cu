@@ -340,42 +340,48 @@ __global__ void __launch_bounds__(kBuildWarps * 32, kBuildBlocksPerSM) build_lis
                 // take the reference's test.
 #if VLJ_BUILD_ORDER == 0
                 // The candidates' group is the outer loop, the homes' counts
-                // in their lanes.
-                for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
-                    const uint32_t q = c0 + lane;
-                    const bool valid = q < staged;
-                    const uint4 e = s_cand[warp][valid ? q : 0u];
-                    const uint32_t e_tix = tiles ? s_tix[warp][valid ? q : 0u] : 0u;
-                    for (uint32_t h = 0; h < homes; h++) {
-                        const uint4 hp = s_home[warp][h];
-                        float r2e;
-                        if (wide) {
-                            const float dx = __uint_as_float(e.x) - __uint_as_float(hp.x);
-                            const float dy = __uint_as_float(e.y) - __uint_as_float(hp.y);
-                            const float dz = __uint_as_float(e.z) - __uint_as_float(hp.z);
-                            r2e = dx * dx + dy * dy + dz * dz;
-                        } else {
-                            r2e = encoded_r2(e, hp, dec);
+                // in their lanes; one loop for each form of the separation.
+                auto test_groups = [&](auto r2_of) {
+                    for (uint32_t c0 = 0; c0 < staged; c0 += 32) {
+                        const uint32_t q = c0 + lane;
+                        const bool valid = q < staged;
+                        const uint4 e = s_cand[warp][valid ? q : 0u];
+                        const uint32_t e_tix = tiles ? s_tix[warp][valid ? q : 0u] : 0u;
+                        for (uint32_t h = 0; h < homes; h++) {
+                            const uint4 hp = s_home[warp][h];
+                            const float r2e = r2_of(e, hp);
+                            const bool near = valid && r2e < pre_r2 && e.w != hp.w;
+                            bool take = near && r2e < acc_r2;
+                            if (near && !take) take = ref_test(a, bx, hp.w, e.w, s_q510);
+                            const unsigned m = __ballot_sync(0xffffffffu, take);
+                            if (m == 0u) continue;
+                            // entry k of the home particle's list: row k / 4, place k % 4
+                            const uint32_t k = __shfl_sync(0xffffffffu, found, h) +
+                                               (uint32_t)__popc(m & below);
+                            store_if(take && k < cap,
+                                     a.list + ((unsigned long long)(k >> 2) * row_stride +
+                                               (hp.w * 4u + (k & 3u))),
+                                     e.w);
+                            // entry k of the 16-bit list of the home's sorted
+                            // position h0 + h: row k / 8, place k % 8
+                            if (tiles)
+                                store16_if(take && k < cap,
+                                           a.list16 + ((unsigned long long)(k >> 3) * row16_stride +
+                                                       ((h0 + h) * 8u + (k & 7u))),
+                                           e_tix);
+                            if (lane == h) found += (uint32_t)__popc(m);
                         }
-                        const bool near = valid && r2e < pre_r2 && e.w != hp.w;
-                        bool take = near && r2e < acc_r2;
-                        if (near && !take) take = ref_test(a, bx, hp.w, e.w, s_q510);
-                        const unsigned m = __ballot_sync(0xffffffffu, take);
-                        if (m == 0u) continue;
-                        const uint32_t k = __shfl_sync(0xffffffffu, found, h) +
-                                           (uint32_t)__popc(m & below);
-                        store_if(take && k < cap,
-                                 a.list + ((unsigned long long)(k >> 2) * row_stride +
-                                           (hp.w * 4u + (k & 3u))),
-                                 e.w);
-                        if (tiles)
-                            store16_if(take && k < cap,
-                                       a.list16 + ((unsigned long long)(k >> 3) * row16_stride +
-                                                   ((h0 + h) * 8u + (k & 7u))),
-                                       e_tix);
-                        if (lane == h) found += (uint32_t)__popc(m);
                     }
-                }
+                };
+                if (wide)
+                    test_groups([](const uint4& e, const uint4& hp) {
+                        const float dx = __uint_as_float(e.x) - __uint_as_float(hp.x);
+                        const float dy = __uint_as_float(e.y) - __uint_as_float(hp.y);
+                        const float dz = __uint_as_float(e.z) - __uint_as_float(hp.z);
+                        return dx * dx + dy * dy + dz * dz;
+                    });
+                else
+                    test_groups([&](const uint4& e, const uint4& hp) { return encoded_r2(e, hp, dec); });
 #else
                 // The home is the outer loop: its position and its count so
                 // far sit in warp-uniform registers for all its groups.
