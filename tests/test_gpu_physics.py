@@ -104,13 +104,15 @@ def test_nose_hoover_samples_the_canonical_ensemble(gpu):
     dof = 3 * n - 3
     start = sim.measure_now()
     temps, times, extended = [], [], []
-    for _ in range(2000):
+    # 10,000 samples 0.04 apart: the temperature decorrelates over about the
+    # thermostat period (0.5), so some 800 of them are independent and the
+    # variance ratio's standard error is about 5 %
+    for _ in range(10_000):
         sim.run(20)
         m = sim.measure_now()
         temps.append(m.temperature(dof))
         times.append(m.time)
         extended.append(m.extended_energy())
-    end = sim.measure_now()
     temps = np.array(temps)
     mean = float(temps.mean())
     ratio = float(temps.var(ddof=1)) / mean ** 2
@@ -118,11 +120,14 @@ def test_nose_hoover_samples_the_canonical_ensemble(gpu):
     # The reference takes end minus start; the extended energy of this
     # splitting fluctuates by about 1e-4 at dt 0.002 (the f64 oracle's own run
     # of this system swings by up to 1.9e-4 between samples), so the drift is
-    # the least-squares slope over the 2000 samples, times the duration, held to
-    # the same bound.
+    # the least-squares slope over the first 2000 samples (80 time units),
+    # times their duration, held to the same bound.
+    times, extended = times[:2000], extended[:2000]
+    end_e = extended[-1]
+    end = sim.measure_now()
     slope = np.polyfit(np.array(times), np.array(extended), 1)[0]
     drift = slope * (times[-1] - times[0]) / abs(start.extended_energy())
-    print(f"end minus start {(end.extended_energy() - start.extended_energy()) / abs(start.extended_energy()):.2e}")
+    print(f"end minus start {(end_e - start.extended_energy()) / abs(start.extended_energy()):.2e}")
     print(f"mean T {mean:.4f}; Var/T^2 {ratio:.3e} vs {canonical:.3e}; drift {drift:.2e}")
     assert abs(mean / temperature - 1.0) < 0.01
     assert abs(ratio / canonical - 1.0) < 0.15
@@ -167,12 +172,20 @@ def coexistence(gpu, shifted_force, blocks):
     return out
 
 
+# Blocks of 20,000 steps (100 time units) next to each other are correlated
+# through the slab's slow modes (interface positions, capillary waves), so
+# the error comes from the means of groups of this many consecutive blocks.
+COEXISTENCE_GROUP = 4
+
+
 def summary(blocks, key, k=None):
-    return mean_error([b[key] if k is None else b[key][k] for b in blocks])
+    x = np.asarray([b[key] if k is None else b[key][k] for b in blocks], dtype=np.float64)
+    g = COEXISTENCE_GROUP if len(x) % COEXISTENCE_GROUP == 0 and len(x) >= 3 * COEXISTENCE_GROUP else 1
+    return mean_error(x.reshape(-1, g).mean(axis=1))
 
 
 def test_force_shifted_slab_coexists_at_nist_densities(gpu):
-    blocks = coexistence(gpu, True, 10)
+    blocks = coexistence(gpu, True, 40)
     liquid, vapour = summary(blocks, "liquid"), summary(blocks, "vapour")
     p_n, t = summary(blocks, "normal"), summary(blocks, "temperature")
     regions = [summary(blocks, "by_region", k) for k in range(3)]
@@ -181,21 +194,33 @@ def test_force_shifted_slab_coexists_at_nist_densities(gpu):
     nist_liquid, nist_liquid_95 = 0.729309, 1.93161e-4
     nist_vapour, nist_vapour_95 = 1.95113e-2, 1.67304e-6
     nist_p, nist_p_95 = 1.18969e-2, 8.67525e-7
+    # The reference's own run of this slab (docs/VALIDATION.md:70): its liquid
+    # sits 1.7 of its standard errors below NIST (the finite slab), and
+    # independent runs of it scatter by about those errors, so they are the
+    # least standard error a run is held to.
+    ref_liquid, ref_vapour, ref_p = (0.72864, 0.00038), (0.01956, 0.00033), (0.011876, 0.000116)
 
-    def agrees(m, reference, limit95):
+    def agrees(m, reference, limit95, floor=0.0):
         x, e = m
+        e = max(e, floor)
         return abs(x - reference) < 3.0 * math.sqrt(e * e + (limit95 / 2.0) ** 2)
 
+    def matches_reference(m, r):
+        return abs(m[0] - r[0]) < 3.0 * math.sqrt(m[1] ** 2 + r[1] ** 2)
+
     assert abs(t[0] - 0.7) < 0.002
-    assert agrees(liquid, nist_liquid, nist_liquid_95)
-    assert agrees(vapour, nist_vapour, nist_vapour_95)
-    assert agrees(p_n, nist_p, nist_p_95)
+    assert agrees(liquid, nist_liquid, nist_liquid_95, ref_liquid[1])
+    assert agrees(vapour, nist_vapour, nist_vapour_95, ref_vapour[1])
+    assert agrees(p_n, nist_p, nist_p_95, ref_p[1])
+    assert matches_reference(liquid, ref_liquid)
+    assert matches_reference(vapour, ref_vapour)
+    assert matches_reference(p_n, ref_p)
     for region in regions:
         assert agrees(region, p_n[0], 2.0 * p_n[1]), "normal pressure not flat"
 
 
 def test_truncated_shifted_slab_has_published_surface_tension(gpu):
-    blocks = coexistence(gpu, False, 10)
+    blocks = coexistence(gpu, False, 40)
     gamma, t = summary(blocks, "gamma"), summary(blocks, "temperature")
     # Vrabec, Kedia, Fuchs and Hasse, Mol. Phys. 104, 1509 (2006)
     published = 2.08 * (1.0 - 0.7 / 1.0779) ** 1.21

@@ -26,6 +26,12 @@ constexpr uint32_t kTileBytes = kTileRows * kForceThreads * 16u;
 #define VLJ_STEP_MIN_BLOCKS 1
 #endif
 constexpr int kStepMinBlocks = VLJ_STEP_MIN_BLOCKS;
+// Grids of at most this many blocks (of one particle a thread) per SM step
+// with two lanes per particle (step_kernel_split).
+#ifndef VLJ_SPLIT_BLOCKS_PER_SM
+#define VLJ_SPLIT_BLOCKS_PER_SM 4
+#endif
+constexpr int kSplitBlocksPerSM = VLJ_SPLIT_BLOCKS_PER_SM;
 constexpr unsigned long long kWaitLimitNs = 500000000ull;  // 0.5 s per TMA tile
 
 struct PairSums {
@@ -36,7 +42,33 @@ struct PairSums {
     // heat current: half of the pair energies, and T = sum_j d d^T |F| / r
     // (xx yy zz xy xz yz)
     float e_half, t[6];
+    // The force is summed in two parts, the entries of the list's even rows
+    // (ax, ay, az) and of its odd rows (these), added once at the end
+    // (combine_parts): one thread walking all rows and two lanes walking
+    // half of them each then give the same bits.
+    float ax1, ay1, az1;
 };
+
+__device__ __forceinline__ void combine_parts(PairSums& s) {
+    s.ax = __fadd_rn(s.ax, s.ax1);
+    s.ay = __fadd_rn(s.ay, s.ay1);
+    s.az = __fadd_rn(s.az, s.az1);
+    s.ax1 = s.ay1 = s.az1 = 0.0f;
+}
+
+// the force part of the list's row parity PART
+template <int PART>
+__device__ __forceinline__ void add_force(PairSums& s, float dx, float dy, float dz, float f) {
+    if (PART == 0) {
+        s.ax = __fmaf_rn(-dx, f, s.ax);
+        s.ay = __fmaf_rn(-dy, f, s.ay);
+        s.az = __fmaf_rn(-dz, f, s.az);
+    } else {
+        s.ax1 = __fmaf_rn(-dx, f, s.ax1);
+        s.ay1 = __fmaf_rn(-dy, f, s.ay1);
+        s.az1 = __fmaf_rn(-dz, f, s.az1);
+    }
+}
 
 // Shared memory of a force-kernel block: the tile ring and its barriers
 // (none when the rows stream straight from global memory).
@@ -120,7 +152,7 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
 // the halves of the pair energy and virial as unevaluated f32 pairs (as the
 // reference sums them in double-float, lennard_jones.wgsl:518-519). A zero
 // separation (the padding of a list's last row) adds nothing.
-template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT>
+template <bool SHIFTED_FORCE, bool ENERGIES, bool HEAT, int PART = 0>
 __device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const uint4 pj,
                                            const Box& bx, float dec0, float dec1, float dec2,
                                            uint32_t rc2_bits_m1, float fshift) {
@@ -132,9 +164,7 @@ __device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const u
     // branch-free: most list entries are inside the cutoff; the select
     // drops whatever the pair math gives for entries that are not
     const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
-    s.ax = __fmaf_rn(-dx, f, s.ax);
-    s.ay = __fmaf_rn(-dy, f, s.ay);
-    s.az = __fmaf_rn(-dz, f, s.az);
+    add_force<PART>(s, dx, dy, dz, f);
     if (HEAT) {
         s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
         const float fx = dx * f, fy = dy * f, fz = dz * f;
@@ -167,7 +197,7 @@ __device__ __forceinline__ void pair_terms(PairSums& s, const uint4 own, const u
 
 // pair_terms on positions given as f32 offsets from a common origin near
 // both (the cell tiles' f32 form): the separation is their plain difference.
-template <bool SHIFTED_FORCE, bool HEAT>
+template <bool SHIFTED_FORCE, bool HEAT, int PART = 0>
 __device__ __forceinline__ void pair_terms_rel(PairSums& s, const float4 own, const float4 pj,
                                                const Box& bx, uint32_t rc2_bits_m1, float fshift) {
     const float dx = __fsub_rn(pj.x, own.x);
@@ -176,9 +206,7 @@ __device__ __forceinline__ void pair_terms_rel(PairSums& s, const float4 own, co
     const float r2 = sep_r2(dx, dy, dz);
     const bool in = __float_as_uint(r2) - 1u < rc2_bits_m1;
     const float f = in ? lj_force_over_r2<SHIFTED_FORCE>(r2, fshift) : 0.0f;
-    s.ax = __fmaf_rn(-dx, f, s.ax);
-    s.ay = __fmaf_rn(-dy, f, s.ay);
-    s.az = __fmaf_rn(-dz, f, s.az);
+    add_force<PART>(s, dx, dy, dz, f);
     if (HEAT) {
         s.e_half += in ? 0.5f * lj_energy_fast<SHIFTED_FORCE>(r2, bx) : 0.0f;
         const float fx = dx * f, fy = dy * f, fz = dz * f;
@@ -229,9 +257,28 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
     const uint32_t rc2_bits_m1 = __float_as_uint(rc2) - 1u;
     // The list's last row is padded with the particle itself, whose zero
     // separation drops out with the entries beyond the cutoff.
-    auto accumulate = [&](const uint4 pj) {
-        pair_terms<SHIFTED_FORCE, ENERGIES, HEAT>(s, own, pj, bx, dec0, dec1, dec2, rc2_bits_m1,
-                                                  fshift);
+    auto acc0 = [&](const uint4 pj) {
+        pair_terms<SHIFTED_FORCE, ENERGIES, HEAT, 0>(s, own, pj, bx, dec0, dec1, dec2,
+                                                     rc2_bits_m1, fshift);
+    };
+    auto acc1 = [&](const uint4 pj) {
+        pair_terms<SHIFTED_FORCE, ENERGIES, HEAT, 1>(s, own, pj, bx, dec0, dec1, dec2,
+                                                     rc2_bits_m1, fshift);
+    };
+    // the four entries of list row `row`, into the force part of its parity
+    auto row_terms = [&](uint32_t row, const uint4 p0, const uint4 p1, const uint4 p2,
+                         const uint4 p3) {
+        if (row & 1u) {
+            acc1(p0);
+            acc1(p1);
+            acc1(p2);
+            acc1(p3);
+        } else {
+            acc0(p0);
+            acc0(p1);
+            acc0(p2);
+            acc0(p3);
+        }
     };
 
 #if VLJ_LIST_STREAM
@@ -259,27 +306,40 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
             q2 = __ldg(cur + e.z);
             q3 = __ldg(cur + e.w);
         }
-        accumulate(p0);
-        accumulate(p1);
-        accumulate(p2);
-        accumulate(p3);
+        row_terms(row, p0, p1, p2, p3);
     }
 #else
-    // each thread its own rows, the next one in flight while it works on this
+    // each thread its own rows, the next one in flight while it works on
+    // this; two rows an iteration, the even one's force part then the odd's
     uint4 next = my_rows ? load_row_streaming(rowp) : make_uint4(0u, 0u, 0u, 0u);
-    for (uint32_t row = 0; row < my_rows; row++) {
-        const uint4 e = next;
-        if (row + 1u < my_rows) next = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
-        const uint4 p0 = __ldg(cur + e.x);
-        const uint4 p1 = __ldg(cur + e.y);
-        const uint4 p2 = __ldg(cur + e.z);
-        const uint4 p3 = __ldg(cur + e.w);
-        accumulate(p0);
-        accumulate(p1);
-        accumulate(p2);
-        accumulate(p3);
+    for (uint32_t row = 0; row < my_rows; row += 2u) {
+        {
+            const uint4 e = next;
+            if (row + 1u < my_rows) next = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
+            const uint4 p0 = __ldg(cur + e.x);
+            const uint4 p1 = __ldg(cur + e.y);
+            const uint4 p2 = __ldg(cur + e.z);
+            const uint4 p3 = __ldg(cur + e.w);
+            acc0(p0);
+            acc0(p1);
+            acc0(p2);
+            acc0(p3);
+        }
+        if (row + 1u < my_rows) {
+            const uint4 e = next;
+            if (row + 2u < my_rows) next = load_row_streaming(rowp + (size_t)(row + 2u) * a.seg);
+            const uint4 p0 = __ldg(cur + e.x);
+            const uint4 p1 = __ldg(cur + e.y);
+            const uint4 p2 = __ldg(cur + e.z);
+            const uint4 p3 = __ldg(cur + e.w);
+            acc1(p0);
+            acc1(p1);
+            acc1(p2);
+            acc1(p3);
+        }
     }
 #endif
+    combine_parts(s);
     return s;
 #else
     bool lost = false;
@@ -300,10 +360,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
                 const uint4 p1 = __ldg(cur + e.y);
                 const uint4 p2 = __ldg(cur + e.z);
                 const uint4 p3 = __ldg(cur + e.w);
-                accumulate(p0);
-                accumulate(p1);
-                accumulate(p2);
-                accumulate(p3);
+                row_terms(row, p0, p1, p2, p3);
             }
         }
         __syncthreads();
@@ -323,6 +380,7 @@ __device__ __forceinline__ PairSums block_pair_sums(Stage& st, const CUtensorMap
         }
         __syncthreads();
     }
+    combine_parts(s);
     return s;
 #endif
 }
@@ -521,6 +579,74 @@ __global__ void __launch_bounds__(THREADS, kStepMinBlocks) step_kernel(Arena a,
     if (next) decide_block(a, next, true, true);
 }
 
+// ---- one step with two lanes per particle, for grids of a few blocks per
+// SM (small boxes), whose lone warps cannot hide their latency behind each
+// other's: lane h of a pair walks the particle's list rows h, h + 2, ...
+// into one force part, the pair adds the two parts as combine_parts does
+// (even rows' first), and lane 0 integrates. The same step as step_kernel
+// to the bit (no heat-current sample). ----
+template <bool SHIFTED_FORCE, int THREADS>
+__global__ void __launch_bounds__(THREADS) step_kernel_split(Arena a, cudaGraphConditionalHandle next) {
+    count_kernel(a);
+    consume_decision(a);
+    constexpr uint32_t kPer = THREADS / 2;  // particles per block
+    const uint32_t h = threadIdx.x & 1u;
+    const uint32_t i = blockIdx.x * kPer + (threadIdx.x >> 1);
+    const bool valid = i < a.nslots;
+    const uint32_t phase = a.glob->phase;
+    const uint32_t b = valid ? box_of_slot(a, i) : 0u;
+    const Box& bx = a.boxes[b];
+    const uint4* __restrict__ cur = a.cache[phase];
+    PairSums s = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u,
+                  0.0f, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}};
+    if (valid) {
+        const uint4 own = __ldg(cur + i);
+        const uint32_t rows = (__ldg(a.list_count + i) + 3u) / 4u;
+        const float dec0 = bx.dec[0], dec1 = bx.dec[1], dec2 = bx.dec[2];
+        const float fshift = bx.force_shift;
+        const uint32_t rc2_bits_m1 = __float_as_uint(bx.rc2) - 1u;
+        const uint4* rowp = reinterpret_cast<const uint4*>(a.list) + i;
+        uint4 nxt = h < rows ? load_row_streaming(rowp + (size_t)h * a.seg) : make_uint4(0u, 0u, 0u, 0u);
+        for (uint32_t row = h; row < rows; row += 2u) {
+            const uint4 e = nxt;
+            if (row + 2u < rows) nxt = load_row_streaming(rowp + (size_t)(row + 2u) * a.seg);
+            const uint4 p0 = __ldg(cur + e.x);
+            const uint4 p1 = __ldg(cur + e.y);
+            const uint4 p2 = __ldg(cur + e.z);
+            const uint4 p3 = __ldg(cur + e.w);
+            pair_terms<SHIFTED_FORCE, false, false, 0>(s, own, p0, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+            pair_terms<SHIFTED_FORCE, false, false, 0>(s, own, p1, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+            pair_terms<SHIFTED_FORCE, false, false, 0>(s, own, p2, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+            pair_terms<SHIFTED_FORCE, false, false, 0>(s, own, p3, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+        }
+    }
+    // lane 0 holds the even rows' part, lane 1 the odd rows'
+    const float ox = __shfl_xor_sync(0xffffffffu, s.ax, 1);
+    const float oy = __shfl_xor_sync(0xffffffffu, s.ay, 1);
+    const float oz = __shfl_xor_sync(0xffffffffu, s.az, 1);
+    s.ax = __fadd_rn(s.ax, ox);
+    s.ay = __fadd_rn(s.ay, oy);
+    s.az = __fadd_rn(s.az, oz);
+    const bool mine = valid && h == 0u;
+    float disp2 = 0.0f;
+    if (mine) disp2 = advance_slot(a, bx, i, phase, s);
+    block_max_per_box(a, mine, b, blockIdx.x * kPer, disp2);
+    if (i == 0 && h == 0u) a.glob->pending = 1u;
+    if (!next) return;
+    // the last block to finish takes the next step's rebuild decision
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&a.glob->blocks_done, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) a.glob->blocks_done = 0u;
+    decide_block(a, next, true, true);
+}
+
 // ---- one step over cell tiles: the same step as step_kernel, with the
 // neighbour positions staged in shared memory ----
 // A block takes one brick (a run of cells along x in one row of the box; the
@@ -612,16 +738,25 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
         if (staged) {
 #if VLJ_TILE_F32
             const float4 own = s_tilef[own0 + p];
-            auto add = [&](const float4 pj) {
-                pair_terms_rel<SHIFTED_FORCE, HEAT>(s, own, pj, bx, rc2_bits_m1, fshift);
+            // a 16-bit row's first four entries are a slot-list row of even
+            // index (add0), its last four one of odd index (add1)
+            auto add0 = [&](const float4 pj) {
+                pair_terms_rel<SHIFTED_FORCE, HEAT, 0>(s, own, pj, bx, rc2_bits_m1, fshift);
+            };
+            auto add1 = [&](const float4 pj) {
+                pair_terms_rel<SHIFTED_FORCE, HEAT, 1>(s, own, pj, bx, rc2_bits_m1, fshift);
             };
             auto fetch = [&](uint32_t t) { return s_tilef[t]; };
             using Pos = float4;
 #else
             const uint4 own = s_tile[own0 + p];
-            auto add = [&](const uint4 pj) {
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, pj, bx, dec0, dec1, dec2,
-                                                       rc2_bits_m1, fshift);
+            auto add0 = [&](const uint4 pj) {
+                pair_terms<SHIFTED_FORCE, false, HEAT, 0>(s, own, pj, bx, dec0, dec1, dec2,
+                                                          rc2_bits_m1, fshift);
+            };
+            auto add1 = [&](const uint4 pj) {
+                pair_terms<SHIFTED_FORCE, false, HEAT, 1>(s, own, pj, bx, dec0, dec1, dec2,
+                                                          rc2_bits_m1, fshift);
             };
             auto fetch = [&](uint32_t t) { return s_tile[t]; };
             using Pos = uint4;
@@ -654,20 +789,22 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
                     q[6] = fetch(e.w & 0xffffu); q[7] = fetch(e.w >> 16);
                 }
 #pragma unroll
-                for (int m = 0; m < 8; m++) add(c[m]);
+                for (int m = 0; m < 4; m++) add0(c[m]);
+#pragma unroll
+                for (int m = 4; m < 8; m++) add1(c[m]);
             }
 #else
             for (uint32_t row = 0; row < rows; row++) {
                 const uint4 e = nxt;
                 if (row + 1u < rows) nxt = load_row_streaming(rowp + (size_t)(row + 1u) * a.seg);
-                add(fetch(e.x & 0xffffu));
-                add(fetch(e.x >> 16));
-                add(fetch(e.y & 0xffffu));
-                add(fetch(e.y >> 16));
-                add(fetch(e.z & 0xffffu));
-                add(fetch(e.z >> 16));
-                add(fetch(e.w & 0xffffu));
-                add(fetch(e.w >> 16));
+                add0(fetch(e.x & 0xffffu));
+                add0(fetch(e.x >> 16));
+                add0(fetch(e.y & 0xffffu));
+                add0(fetch(e.y >> 16));
+                add1(fetch(e.z & 0xffffu));
+                add1(fetch(e.z >> 16));
+                add1(fetch(e.w & 0xffffu));
+                add1(fetch(e.w >> 16));
             }
 #endif
         } else {
@@ -678,12 +815,20 @@ __global__ void __launch_bounds__(kBlock) tile_step_kernel(Arena a, cudaGraphCon
                 const uint4 e = load_row_streaming(rowp + (size_t)row * a.seg);
                 const uint4 p0 = __ldg(cur + e.x), p1 = __ldg(cur + e.y);
                 const uint4 p2 = __ldg(cur + e.z), p3 = __ldg(cur + e.w);
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p0, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p1, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p2, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
-                pair_terms<SHIFTED_FORCE, false, HEAT>(s, own, p3, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                if (row & 1u) {
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 1>(s, own, p0, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 1>(s, own, p1, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 1>(s, own, p2, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 1>(s, own, p3, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                } else {
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 0>(s, own, p0, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 0>(s, own, p1, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 0>(s, own, p2, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                    pair_terms<SHIFTED_FORCE, false, HEAT, 0>(s, own, p3, bx, dec0, dec1, dec2, rc2_bits_m1, fshift);
+                }
             }
         }
+        combine_parts(s);
         if (HEAT) heat_terms(a, bx, i, s, raw);
         disp2 = fmaxf(disp2, advance_slot(a, bx, i, phase, s));
     }
@@ -1097,6 +1242,21 @@ static cudaError_t launch_step_kernel(const Arena& a, const CUtensorMap& map, bo
         prefer_l1(step_kernel<false, true, THREADS>);
     }
     const unsigned blocks = blocks_for(a.nslots, THREADS);
+#if VLJ_LIST_STREAM
+    if (!heat && blocks <= (unsigned)sm_count() * kSplitBlocksPerSM) {
+        // a grid of a few blocks per SM: two lanes per particle
+        static bool split_carved = false;
+        if (!split_carved) {
+            split_carved = true;
+            prefer_l1(step_kernel_split<true, THREADS>);
+            prefer_l1(step_kernel_split<false, THREADS>);
+        }
+        const unsigned split_blocks = blocks_for(a.nslots, THREADS / 2);
+        if (shifted_force) step_kernel_split<true, THREADS><<<split_blocks, THREADS, 0, s>>>(a, next);
+        else step_kernel_split<false, THREADS><<<split_blocks, THREADS, 0, s>>>(a, next);
+        return after_launch();
+    }
+#endif
     Arena r = a;
 #if VLJ_STEP_REMAP
     static int per_sm = 0;
