@@ -35,6 +35,8 @@ def main():
                     help="enqueue steps as direct launches (profilers see each kernel)")
     ap.add_argument("--no-tiles", action="store_true",
                     help="step kernel with per-particle gathers instead of cell tiles")
+    ap.add_argument("--threads", type=int, default=0, choices=(0, 64, 128, 256),
+                    help="particles per block of the step kernel (0: the library's default)")
     ap.add_argument("--record", default=None, metavar="DIR",
                     help="write measurements.csv (a row every --every steps), positions.npy "
                          "and run.json into DIR, in the reference's formats")
@@ -52,6 +54,8 @@ def main():
         sim.set_graphs(False)
     if args.no_tiles:
         sim.set_tiles(False)
+    if args.threads:
+        sim.set_step_threads(args.threads)
     m = sim.measure_now()
     print(f"{len(p)} particles, box {box:.4f}: E {m.energy():.6f} P {m.pressure():.6f}")
     t0 = time.perf_counter()
