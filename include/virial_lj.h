@@ -402,6 +402,12 @@ VLJ_API vlj_status vlj_debug_set_tiles(vlj_sim *sim, int on);
  * tuning knob: virial_lj.tune_batch times it per replica set; the same
  * trajectory to the bit). */
 VLJ_API vlj_status vlj_debug_set_step_threads(vlj_sim *sim, uint32_t threads);
+/* Lanes per particle of the step kernel: 0 (the default) chooses by grid
+ * size (two lanes for grids of a few blocks per SM), 1 or 2 forces one form.
+ * Every kernel sums a particle's force in two parts (the list's even and odd
+ * rows) added once at the end, so the trajectory is the same to the bit
+ * either way; the switch is for tests and timing. */
+VLJ_API vlj_status vlj_debug_set_step_lanes(vlj_sim *sim, uint32_t lanes);
 VLJ_API vlj_status vlj_debug_tile_info(vlj_sim *sim, uint32_t *brick_cols, uint32_t *bricks,
                                        uint32_t *tile_cap, uint32_t *threads);
 VLJ_API vlj_status vlj_debug_read_tile_lists(vlj_sim *sim, uint16_t *out);

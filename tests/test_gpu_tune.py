@@ -1,8 +1,9 @@
 """Run-time choices of the step kernel's form on a single box: the cell
-tiles' bricks per x-row (vlj_set_tile_cols) and the particles per block keep
-the trajectory to the bit, and virial_lj.tune_box times them on a copy of
-the box and returns the fastest."""
+tiles' bricks per x-row (vlj_set_tile_cols), the particles per block and the
+lanes per particle keep the trajectory to the bit, and virial_lj.tune_box
+times them on a copy of the box and returns the fastest."""
 
+import numpy as np
 import pytest
 from test_gpu_tiles import check_tile_lists
 
@@ -85,3 +86,54 @@ def test_tune_box_times_every_form(gpu):
     assert a.read_particles().tobytes() == b.read_particles().tobytes()
     a.close()
     b.close()
+
+
+def lanes_run(gpu, p, st, lanes, steps, heat_every=0):
+    sim = gpu.LennardJones(p, st)
+    sim.set_step_lanes(lanes)
+    if heat_every:
+        sim.record_heat_current(steps // heat_every + 1)
+        for k in range(steps):
+            sim.step(1)
+            if k % heat_every == 0:
+                sim.sample_heat_current()
+    else:
+        sim.run(steps)
+    m = sim.measure_now()
+    out = (sim.read_particles().tobytes(), m.potential, m.virial, m.kinetic, m.list_rebuilds,
+           np.asarray(sim.read_heat_current()).tobytes() if heat_every else None)
+    sim.close()
+    return out
+
+
+@pytest.mark.parametrize("case", ["lattice1000", "fcc20_langevin", "fcc40_langevin"])
+def test_two_lanes_per_particle_keep_the_trajectory(gpu, case):
+    # forces summed in two parts (even and odd list rows) in every kernel:
+    # two lanes a particle and one give the same bits, on a small box (where
+    # two lanes are the default), a mid-size and the 256k box
+    if case == "lattice1000":
+        L = (1000 / 0.8442) ** (1 / 3)
+        p = gpu.lattice(1000, L, 0.72, 1)
+        st = gpu.Settings([L] * 3, dt=0.005)
+        steps = 300
+    else:
+        cells = 20 if case == "fcc20_langevin" else 40
+        p, L = gpu.lattice_fcc(cells, 0.8442, 1.0, 5)
+        st = gpu.Settings([L] * 3, dt=0.005, shifted_force=True,
+                          thermostat=gpu.Langevin(1.0, 1.0, 5))
+        steps = 100
+    one = lanes_run(gpu, p, st, 1, steps)
+    two = lanes_run(gpu, p, st, 2, steps)
+    auto = lanes_run(gpu, p, st, 0, steps)
+    assert one[4] >= 2  # rebuilds on the way
+    assert one == two == auto
+
+
+def test_two_lanes_beside_heat_current_samples(gpu):
+    # steps that take a heat-current sample run the one-lane kernel, the
+    # others two lanes: the same trajectory and series as one lane throughout
+    p, L = gpu.lattice_fcc(12, 0.8442, 0.722, 5)
+    st = gpu.Settings([L] * 3, dt=0.004)
+    one = lanes_run(gpu, p, st, 1, 60, heat_every=3)
+    two = lanes_run(gpu, p, st, 2, 60, heat_every=3)
+    assert one == two

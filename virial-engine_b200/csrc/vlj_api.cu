@@ -856,6 +856,16 @@ vlj_status vlj_set_tile_cols(vlj_sim* s, uint32_t cols) {
     return VLJ_OK;
 }
 
+vlj_status vlj_debug_set_step_lanes(vlj_sim* s, uint32_t lanes) {
+    if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
+    if (lanes > 2u) return fail(VLJ_INVALID_ARG, "step lanes must be 0 (by grid size), 1 or 2");
+    if (lanes == s->arena.step_lanes) return VLJ_OK;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    sim_drop_step_graphs(s);
+    s->arena.step_lanes = lanes;
+    return VLJ_OK;
+}
+
 vlj_status vlj_debug_set_step_threads(vlj_sim* s, uint32_t threads) {
     if (!s) return fail(VLJ_INVALID_ARG, "sim is null");
     if (threads != 64 && threads != 128 && threads != 256)

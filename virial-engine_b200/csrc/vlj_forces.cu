@@ -1243,7 +1243,9 @@ static cudaError_t launch_step_kernel(const Arena& a, const CUtensorMap& map, bo
     }
     const unsigned blocks = blocks_for(a.nslots, THREADS);
 #if VLJ_LIST_STREAM
-    if (!heat && blocks <= (unsigned)sm_count() * kSplitBlocksPerSM) {
+    const bool split = a.step_lanes == 2u ||
+                       (a.step_lanes == 0u && blocks <= (unsigned)sm_count() * kSplitBlocksPerSM);
+    if (!heat && split) {
         // a grid of a few blocks per SM: two lanes per particle
         static bool split_carved = false;
         if (!split_carved) {

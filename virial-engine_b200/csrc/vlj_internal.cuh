@@ -253,6 +253,7 @@ struct Arena {
     uint32_t tile_cap;   // tile entries (16 B each) a block stages in shared memory
     uint32_t tile_threads;  // threads of a tile step block
     uint32_t step_threads;  // particles per block of the step kernel: 64, 128 or 256
+    uint32_t step_lanes;    // lanes per particle of the step kernel: 0 by grid size, 1 or 2
     uint32_t remap_sms, remap_per_sm;  // the step kernel's first-wave block layout (VLJ_STEP_REMAP)
     // per force block (kForceThreads slots), for the TMA tile ring only: rows
     // (four entries each) of the longest list in it, so a block stages only

@@ -520,6 +520,11 @@ class LennardJones:
         """Particles per block of the step kernel (64, 128 or 256)."""
         _check(_lib.vlj_debug_set_step_threads(self._h, int(threads)))
 
+    def set_step_lanes(self, lanes):
+        """Lanes per particle of the step kernel: 0 by grid size, 1 or 2 (same
+        trajectory to the bit)."""
+        _check(_lib.vlj_debug_set_step_lanes(self._h, int(lanes)))
+
     def set_tiles(self, on):
         """Cell tiles in the step kernel on or off (same trajectory either way)."""
         _check(_lib.vlj_debug_set_tiles(self._h, int(bool(on))))

@@ -127,6 +127,7 @@ SIGNATURES = {
                            _vp, _vp, _vp, _vp, _vp],
     "vlj_debug_set_tiles": [_vp, C.c_int],
     "vlj_debug_set_step_threads": [_vp, C.c_uint32],
+    "vlj_debug_set_step_lanes": [_vp, C.c_uint32],
     "vlj_debug_tile_info": [_vp, _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32), _P(C.c_uint32)],
     "vlj_debug_read_tile_lists": [_vp, _vp],
 }
