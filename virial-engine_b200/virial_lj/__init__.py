@@ -792,7 +792,7 @@ def tune_batch(replicas, skins=(0.3, 0.4, 0.5, 0.6, 0.8), threads=(64, 128, 256)
 
 
 def tune_box(particles, settings: Settings, tile_cols=(0, 3, 4, 5, 6), threads=(64, 128, 256),
-             steps=30, warmup=10, flush_bytes=256 << 20, stream=None):
+             steps=30, warmup=10, flush_bytes=256 << 20, stream=None, stats=None):
     """The step kernel's form that steps this box fastest on this GPU: the
     cell tiles' bricks per x-row (0: per-particle gathers, the default) and
     the particles per block of the per-particle kernel.
@@ -804,7 +804,8 @@ def tune_box(particles, settings: Settings, tile_cols=(0, 3, 4, 5, 6), threads=(
     clears the L2 (0: no flush). Tile sizes the box cannot take (too few
     particles per cell, more bricks than cells along x) are skipped. Returns
     (cols, threads, {(cols, threads): seconds per step}); apply them with
-    set_tile_cols and set_step_threads.
+    set_tile_cols and set_step_threads. A dict given as `stats` receives the
+    number of the library's kernels the copy ran ("kernels").
     """
     import torch
 
@@ -835,6 +836,8 @@ def tune_box(particles, settings: Settings, tile_cols=(0, 3, 4, 5, 6), threads=(
                 b.record(s)
             s.synchronize()
             times[(cols, t)] = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / steps
+        if stats is not None:
+            stats["kernels"] = sim.kernels_executed()
     finally:
         sim.close()
     cols, t = min(times, key=times.get)
