@@ -148,7 +148,7 @@ __device__ __forceinline__ bool grid_pass(const Arena& a) {
 // the step counter), then per box: rebuild when something moved more than
 // skin / 2 since the last build, or never built; reorder on every
 // reorder_every-th rebuild (counted before the increment, as the reference).
-// With `set`, the verdict (some box rebuilds) becomes the value of the graph
+// With `set`, the decision (some box rebuilds) becomes the value of the graph
 // conditional `handle`.
 // A step kernel's last block takes the next step's decision itself
 // (`folded`) and leaves Global::decided set; the step that follows consumes
