@@ -61,10 +61,15 @@ def test_rectangular_box_matches_all_pairs(gpu, O, shifted_force):
     assert rel(m.virial, w.sum()) < TOL
 
 
-def compare_rebuild(sim, O, pre, reorder, vel_stored=None):
-    """The sim's current grid and lists against the oracle's rebuild of `pre`."""
+def compare_rebuild(sim, O, pre, reorder, vel_stored=None, grown=False):
+    """The sim's current grid and lists against the oracle's rebuild of `pre`
+    (with `grown`, at the capacity the sim's lists grew to, not the
+    reference's starting capacity)."""
     g = sim.grid_info()
     s = O.setup(np.zeros((sim.count(), 3)), sim.box_size(), 2.5, 0.3, False)
+    if grown:
+        assert g.capacity >= s.capacity
+        s.capacity = g.capacity
     assert list(g.cells) == list(s.cells) and g.capacity == s.capacity
     r = O.rebuild_ref(s, pre["x"], pre["v"], pre["ids"], reorder)
     now = sim.read_grid()
@@ -101,6 +106,39 @@ def test_later_rebuilds_match_reference_bit_for_bit(gpu, O):
         seen.add(reorder)
         compare_rebuild(sim, O, dict(x=pre["x"], v=pre["v"], ids=pre["ids"]), reorder)
     assert seen == {True, False}
+
+
+# name: (atoms, box, lift of the lattice along z, box the lattice fills,
+# temperature, steps before each compared rebuild)
+LIST_CASES = {
+    "dilute_gas_rho0.04": (3000, [42.0, 42.0, 42.0], 0.0, None, 2.0, 120),
+    "dense_liquid_rho0.95": (4000, [16.15] * 3, 0.0, None, 1.5, 60),
+    "elongated_box": (3000, [10.0, 10.0, 40.0], 0.0, None, 1.2, 80),
+    "three_cells_a_side": (500, [8.5] * 3, 0.0, None, 1.0, 80),
+    "liquid_vapour_slab": (16000, [20.0, 20.0, 150.0], 47.6, [20.0, 20.0, 54.8], 0.7, 60),
+}
+
+
+@pytest.mark.parametrize("case", sorted(LIST_CASES))
+def test_lists_bit_exact_across_densities_and_shapes(gpu, O, case):
+    # binning, per-cell order and lists after the box has moved (two forced
+    # rebuilds, reordering or not as the schedule has it), against the
+    # oracle (at the slab's grown capacity if its liquid overflowed the
+    # reference's)
+    n, box, lift, fill, t, steps = LIST_CASES[case]
+    p = gpu.lattice_box(n, fill or box, t, 9)
+    p["pos"][:, 2] += lift
+    sim = gpu.LennardJones(p, gpu.Settings(box, dt=0.005, shifted_force=True,
+                                           thermostat=gpu.Langevin(t, 1.0, 9)))
+    for _ in range(2):
+        sim.run(steps)
+        pre = sim.read_grid()
+        before = sim.grid_info().rebuilds
+        sim.force_rebuild()
+        reorder = before % 4 == 0
+        compare_rebuild(sim, O, dict(x=pre["x"], v=pre["v"], ids=pre["ids"]), reorder,
+                        grown=case == "liquid_vapour_slab")
+    sim.close()
 
 
 def test_fixed_point_totals_are_exact(gpu, O):
