@@ -89,7 +89,10 @@ constexpr uint32_t kDenseCell = 8;  // particles in a cell the list build takes 
 // home particles split into parts of kPartHomes (at most kMaxParts, the
 // last taking the rest), each a work-list entry of its own: entry = cell * 8
 // + part.
-constexpr uint32_t kPartHomes = 8;
+#ifndef VLJ_PART_HOMES
+#define VLJ_PART_HOMES 8
+#endif
+constexpr uint32_t kPartHomes = VLJ_PART_HOMES;
 constexpr uint32_t kMaxParts = 8;
 constexpr int kTileRows = VLJ_TILE_ROWS;
 constexpr int kTileSlots = VLJ_TILE_SLOTS;  // tiles in flight per block
