@@ -70,3 +70,25 @@ def test_create_without_device_fails_loudly(vl):
     with pytest.raises(vl.VljError) as e:
         vl.LennardJones(p, vl.Settings([11.0] * 3))
     assert e.value.status == "NO_DEVICE"
+
+
+def header_arities():
+    """Parameter count of every function the header declares."""
+    text = open(os.path.join(ROOT, "include", "virial_lj.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"VLJ_API\s+[\w\s\*]+?\b(vlj_\w+)\s*\(([^)]*)\)", text):
+        args = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_python_signatures_match_the_header():
+    # the ctypes table passes exactly the arguments each C function takes
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "virial-engine_b200"))
+    from virial_lj import _ffi
+    arity = header_arities()
+    assert set(_ffi.SIGNATURES) <= set(arity), sorted(set(_ffi.SIGNATURES) - set(arity))
+    wrong = {n: (len(t), arity[n]) for n, t in _ffi.SIGNATURES.items() if len(t) != arity[n]}
+    assert not wrong, wrong
