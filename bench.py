@@ -679,9 +679,8 @@ def run_ours(args, world, rank, gpu_index):
             "clocks": clk,
             "gpu_launches": launches,
             # this library's kernels that ran before the timed steps (the
-            # tuner's copy of the box, then the box's creation and warm-up):
-            # the launch list of the timed steps is
-            # ncu --kernel-name-base demangled -k regex:vlj:: -s <this> -c <gpu_launches>
+            # tuner's copy of the box, then the box's creation and warm-up),
+            # counted on the device (graph nodes included)
             "kernels_before_timed": tune_stats.get("kernels", 0) + k0,
             "list_rebuilds_timed": rebuilds,
             "check": {"potential": meas.potential, "virial": meas.virial,
